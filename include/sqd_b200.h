@@ -1,0 +1,159 @@
+/*
+ * sqd_b200.h — C ABI of the B200 (sm_100a) implementation of the sample-based quantum
+ * diagonalization (SQD) hot path of rqutils: Pauli-sum preprocessing, subspace build, the
+ * matrix-free Pauli-sum matvec over a sorted subspace of computational-basis bitstrings, and the
+ * single-vector LOCG/LOBPCG ground-state solver that drives it.
+ *
+ * Conventions
+ *  - Every array argument is a DEVICE pointer unless its name ends in `_host`.  The library never
+ *    frees memory it did not allocate.  Opaque handles own the tables they build (allocated
+ *    stream-ordered on the stream passed at creation) and are released with *_destroy.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).  All work is
+ *    stream-ordered; functions that return host scalars synchronize that stream.
+ *  - Return value: SQD_OK (0) or a negative status; sqd_last_error() gives the message of the
+ *    last failure on the calling thread.  No C++ exception crosses the ABI.
+ *  - A state is a uint64 whose bit q is qubit q (num_qubits <= 63).  A Pauli term is a pair of
+ *    uint64 masks (x, z): X on qubits with x=1,z=0, Y on x=1,z=1, Z on x=0,z=1.
+ *  - Vector dtypes: SQD_F64, SQD_C128 (interleaved re/im doubles), SQD_F32, SQD_C64.
+ *
+ * The rqutils functions each entry point replaces are cited as path:line within rqutils.
+ */
+#ifndef SQD_B200_H
+#define SQD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum sqd_status {
+  SQD_OK = 0,
+  SQD_ERR_INVALID = -1,    /* bad argument (maps to ValueError) */
+  SQD_ERR_CUDA = -2,       /* CUDA runtime error */
+  SQD_ERR_UNSUPPORTED = -3,
+  SQD_ERR_DEVICE = -4,     /* a kernel reported an error through its device status word */
+  SQD_ERR_MEMORY = -5
+};
+
+enum sqd_dtype { SQD_F64 = 0, SQD_C128 = 1, SQD_F32 = 2, SQD_C64 = 3 };
+
+/* Flags for sqd_paulis_create. */
+#define SQD_PAULIS_FORCE_REAL 1u
+
+/* Lookup methods for the b XOR x search. */
+enum sqd_lookup { SQD_LOOKUP_HASH = 0, SQD_LOOKUP_BSEARCH = 1 };
+
+typedef struct sqd_paulis_s* sqd_paulis_t;
+typedef struct sqd_space_s* sqd_space_t;
+typedef struct sqd_op_s* sqd_op_t;
+
+/* ---------------------------------------------------------------- library ------------------ */
+const char* sqd_version(void);
+const char* sqd_last_error(void);
+
+/* ---------------------------------------------------------------- Pauli sums --------------- */
+/* PauliSumXZ.from_paulisum (paulis/symplectic.py:50-124), on the device: drops zero
+ * coefficients, merges duplicate (x, z) terms, groups by X mask (groups ascending in x, terms
+ * ascending in z within a group — the reference's np.unique order), multiplies in the phase
+ * (-i)^{popcount(x & z)}, and optionally keeps only real parts (force_real).  coef_im may be
+ * NULL.  *imag_dropped_host (may be NULL) is set to 1 when force_real discarded a nonzero
+ * imaginary part (the reference warns, symplectic.py:93-94). */
+int sqd_paulis_create(const uint64_t* x, const uint64_t* z, const double* coef_re,
+                      const double* coef_im, int64_t num_raw_terms, int num_qubits,
+                      uint32_t flags, void* stream, sqd_paulis_t* out, int* imag_dropped_host);
+/* The grouped table as the reference stores it (PauliSumXZ fields x, z, c; symplectic.py:41-48)
+ * in CSR form: J groups, M merged terms, K_max = largest group. */
+int sqd_paulis_info(sqd_paulis_t p, int64_t* num_groups, int64_t* num_terms, int64_t* max_k,
+                    int* is_complex, int* num_qubits);
+/* group_x[J], group_start[J+1] (int64), term_z[M], term_c[2M] (interleaved re/im), and
+ * raw_to_term[num_raw] (int32, -1 for dropped zero coefficients). */
+int sqd_paulis_export(sqd_paulis_t p, uint64_t* group_x, int64_t* group_start, uint64_t* term_z,
+                      double* term_c, int32_t* raw_to_term, void* stream);
+void sqd_paulis_destroy(sqd_paulis_t p);
+
+/* ---------------------------------------------------------------- subspace ----------------- */
+/* np.packbits(np.pad(states,...)) of sqd.py:255 in the uint64 representation: bits[n_rows,
+ * num_qubits] (uint8 0/1, last column = qubit 0, row-major) -> uint64 values. */
+int sqd_pack_states(const uint8_t* bits, int64_t n_rows, int num_qubits, uint64_t* out,
+                    void* stream);
+/* uniquify_states (sqd.py:445-482): sorts and de-duplicates n_in states, keeps states_size >=
+ * n_unique vector slots (the tail are fill-in slots), and builds the lookup structures. */
+int sqd_space_create(const uint64_t* states, int64_t n_in, int num_qubits, int64_t states_size,
+                     void* stream, sqd_space_t* out);
+int sqd_space_info(sqd_space_t s, int64_t* n_unique, int64_t* states_size, int* num_sectors,
+                   uint64_t* sector_masks_host /* [2] */);
+/* Sorted unique states (n_unique values). */
+int sqd_space_states(sqd_space_t s, uint64_t* out, void* stream);
+/* get_xsource (sqd.py:485-548), sorted input: out[states_size] = index j with S[j] == S[i]^x,
+ * else -1; fill-in slots get exactly the values the reference's sort-based algorithm gives. */
+int sqd_xsource(sqd_space_t s, uint64_t x, int lookup, int32_t* out, void* stream);
+void sqd_space_destroy(sqd_space_t s);
+
+/* ---------------------------------------------------------------- operator ----------------- */
+/* The operator H projected on the subspace, with a connectivity cache chosen by
+ * cache_strategy (SQDOptions.cache_strategy, sqd.py:187-189, run_sqd sqd.py:343-404):
+ *   x_cache = 1: sources cached (sparse: only (row, group) pairs whose source exists);
+ *   x_cache = 0: sources searched inside every matvec;
+ *   z_cache = 2: matrix elements (composed diagonals) cached per stored pair;
+ *   z_cache = 0 or 1: diagonals recomputed from popcounts inside every matvec.
+ * lookup = enum sqd_lookup. */
+int sqd_op_create(sqd_paulis_t p, sqd_space_t s, int x_cache, int z_cache, int lookup,
+                  void* stream, sqd_op_t* out);
+/* nnz = stored (row, group) pairs (0 when x_cache = 0); value_complex = 1 if H has complex
+ * matrix elements. */
+int sqd_op_info(sqd_op_t op, int64_t* nnz, int64_t* states_size, int* value_complex);
+/* Tuning knob of the cached matvec (no rqutils counterpart; rqutils leaves the schedule to
+ * XLA): lanes of a warp that share one output row, 1/2/4/8/16/32.  Chosen from the mean row
+ * length at creation; the autotuner overrides it. */
+int sqd_op_set_lanes(sqd_op_t op, int lanes_per_row);
+int sqd_op_get_lanes(sqd_op_t op, int* lanes_per_row);
+/* Hv on the subspace (apply_h_x_cached and friends, sqd.py:643-743 via
+ * make_x_cached_matvec sqd.py:746-751).  v and out have states_size elements of dtype. */
+int sqd_matvec(sqd_op_t op, const void* v, void* out, int dtype, void* stream);
+/* Composed diagonal of group j (get_diagonal, sqd.py:603-628) for every slot (fill-in slots use
+ * the all-ones state, as the reference's 255 rows do).  dtype SQD_F64 or SQD_C128. */
+int sqd_diagonal(sqd_op_t op, int64_t group, void* out, int dtype, void* stream);
+/* vinit of run_sqd (sqd.py:406-426): argmin of the real group-0 diagonal over real rows when
+ * group 0 has x = 0, else 0. */
+int sqd_vinit(sqd_op_t op, int64_t* index_host, void* stream);
+/* Projected matrix <i|H|j> in CSR (hproj, sqd.py:269-314, with its padding bug fixed):
+ * indptr[states_size+1] (int64), indices[nnz] (int32), data[nnz] complex128 (interleaved). */
+int sqd_op_csr(sqd_op_t op, int64_t* indptr, int32_t* indices, double* data, void* stream);
+/* Hellmann-Feynman per-term reduction g_t = Re <u| P_t |v> for every merged term t (P_t the
+ * t-th Pauli string with unit coefficient, projected), FP64; u, v of dtype (SQD_F64/C128). */
+int sqd_grad_terms(sqd_op_t op, const void* u, const void* v, int dtype, double* out_terms,
+                   void* stream);
+void sqd_op_destroy(sqd_op_t op);
+
+/* ---------------------------------------------------------------- LOCG --------------------- */
+/* y = A x for a caller-defined operator; must be stream-ordered on `stream`. */
+typedef int (*sqd_matvec_fn)(void* ctx, const void* x, void* y, void* stream);
+
+/* Matvec callback that applies an sqd_op_t passed as ctx (dtype fixed at solver creation). */
+int sqd_op_matvec_cb(void* ctx, const void* x, void* y, void* stream);
+
+enum sqd_locg_mode {
+  SQD_LOCG_FP64 = 0,      /* faithful FP64 restatement of ground_locg */
+  SQD_LOCG_MIXED = 1      /* FP32 inner sweeps + FP64 residual / Rayleigh-Ritz refinement */
+};
+
+/* ground_locg (ground_locg.py:128-162 -> _ground_locg_callable :188-423).
+ *  n, dtype: vector space (SQD_F64 or SQD_C128 for the result).
+ *  fn/ctx: the operator; for SQD_LOCG_MIXED ctx must be an sqd_op_t and fn sqd_op_matvec_cb.
+ *  xinit: start vector (device, dtype) or NULL for the one-hot vector at xinit_index.
+ *  orth/n_orth: device vectors to orthogonalize against (ground_locg `orth`), n_orth <= 8.
+ *  tol < 0 selects the dtype epsilon (:224-225).
+ *  use_graph: capture each iteration in a CUDA graph (only with fn == sqd_op_matvec_cb).
+ *  Outputs: eigval_host, eigvec (device, n elements of dtype), niter_host, and
+ *  residual_host = final |r| (may be NULL). */
+int sqd_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xinit,
+             int64_t xinit_index, const void* const* orth, int n_orth, double tol, int maxiter,
+             int mode, int use_graph, void* stream, double* eigval_host, void* eigvec,
+             int* niter_host, double* residual_host);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SQD_B200_H */

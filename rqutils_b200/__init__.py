@@ -1,0 +1,15 @@
+"""B200-native (sm_100a) implementation of the sample-based quantum diagonalization hot path of
+rqutils: Pauli-sum preprocessing, subspace build, the matrix-free Pauli-sum matvec over a sorted
+subspace of computational-basis bitstrings, and the single-vector LOCG/LOBPCG ground-state
+solver — all as CUDA kernels behind the C ABI in ``include/sqd_b200.h``.
+"""
+from . import _lib
+from .paulis.symplectic import PauliSumXZ
+from .sqd import (SQDOptions, SQDOperator, Subspace, sqd, run_sqd, hproj, uniquify_states,
+                  get_xsource, get_diagonal)
+from .ground_locg import ground_locg
+
+_lib.load()
+
+__all__ = ['PauliSumXZ', 'SQDOptions', 'SQDOperator', 'Subspace', 'sqd', 'run_sqd', 'hproj',
+           'uniquify_states', 'get_xsource', 'get_diagonal', 'ground_locg']

@@ -1,0 +1,869 @@
+// Single-vector LOCG/LOBPCG on the device: ground_locg (ground_locg.py:128-162) and
+// _ground_locg_callable (:188-423), with _project_out (:426-464), eigenpair_2x2 (:467-478) and
+// eigenpair_3x3 (:481-514).
+//
+// Every BLAS-1 step of an iteration is one pass of a fused kernel k_lc: up to two outputs that
+// are linear combinations of up to MAXS input vectors (coefficients read from device memory),
+// plus up to MAXD inner products of inputs/outputs, reduced deterministically (per-block
+// partials, last block sums them in a fixed order).  The last block then runs the scalar step
+// that follows in the algorithm (normalisation factors, the 2x2/3x3 Rayleigh-Ritz solve, the
+// convergence test) on one thread and writes the next pass's coefficients, so an iteration has
+// no host synchronisation.  With an sqd operator as the matvec the whole while-loop is one
+// CUDA graph with a conditional WHILE node whose condition the convergence step sets.
+//
+// Inner products always accumulate in FP64 (also for FP32 vectors).
+#include "internal.cuh"
+#include "dispatch.cuh"
+
+namespace sqd {
+namespace {
+
+constexpr int LC_THREADS = 256;
+constexpr int kMaxOrth = 8;
+
+enum Post : int {
+  P_NONE = 0,
+  P_INV_NORM,        // coef[0][0] = 1/|v| (no zero guard: xinit /= norm)
+  P_THETA0,          // theta = Re <x|ax>; coef (1, -theta) for (ax, x)
+  P_R0NORM,          // rnorm; coef[0][0] = 1/rnorm
+  P_RR2,             // 2x2 Rayleigh-Ritz -> theta, kappa; coefs of t, u over (x, p)
+  P_TU_NORM,         // coefs x = u/|u|, y = t/|t| over (u, t); then r coef (1, -theta)
+  P_PROJ_IPS,        // coef (1, -<x|v>, -<y|v>) over (v, x, y)
+  P_PROJ_NORM_IPS,   // s = 1/|v| (0 -> 1): coef (s, -s<x|v>, -s<y|v>)
+  P_PROJ_MASK,       // keep = |v| >= 0.99
+  P_RR3,             // 3x3 Rayleigh-Ritz -> theta, kappa; coef of s over (x, y, p)
+  P_SNORM,           // |s| -> coefs of u (out0) and t (out1) over (x, y, p)
+  P_XY_NORM,         // coefs x/|u|, y/|t| over (x, y)
+  P_CONV,            // residual test (red0 = |r|^2, red1 = |Ax|^2)
+  P_CONV_SPLIT,      // residual test with |Ax|^2 stored earlier (orth path)
+  P_STORE_AX,        // store |Ax|^2
+  P_ORTH_IPS,        // coef (1, -<o_k|v>...) over (v, o_0, ...)
+  P_ORTH_NORM,       // s = 1/|v| (0 -> 1)
+  P_SET_R_COEF,      // coef (1, -theta) for r = ax - theta x
+  P_THETA_ONLY       // theta = Re <x|ax> (refinement bookkeeping)
+};
+
+struct LocgDev {
+  double red[16][2];     // reduction results of the last pass
+  double coef[2][10][2]; // coefficients of the next pass
+  double theta;
+  double theta_prev;
+  double kappa[3][2];
+  double rnorm;
+  double axnorm2;
+  double tol;
+  double nscale;         // 10 * n (reltol factor)
+  double inner_rtol;     // > 0: converge on |r| < inner_rtol |theta| (FP32 inner sweeps)
+  double etol;           // > 0: also stop when |dtheta| <= etol |theta|
+  double best_r;
+  int best_it;
+  int niter;
+  int maxiter;
+  int converged;
+  int done;
+  int keep;              // project_out mask result
+  int rzero;
+  int stall;             // stop after this many iterations without improving |r| (0 = never)
+};
+
+enum Gate : int { G_NONE = 0, G_DONE = 1, G_KEEP = 2 };
+
+template <int MAXS, int MAXD>
+struct LCArgs {
+  int64_t n;
+  const void* src[MAXS];
+  void* out[2];
+  int nsrc, nout, ndot, post, gate, use_cond;
+  signed char da[MAXD], db[MAXD];
+  LocgDev* dev;
+  double* partials;
+  unsigned* counter;
+  cudaGraphConditionalHandle cond;
+};
+
+// ----------------------------------------------------------------------------- small solvers
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
+__device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+  const double d = b.x * b.x + b.y * b.y;
+  return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+__device__ __forceinline__ double2 csub(double2 a, double2 b) {
+  return make_double2(a.x - b.x, a.y - b.y);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ double2 cscale(double2 a, double s) {
+  return make_double2(a.x * s, a.y * s);
+}
+
+// eigenpair_2x2 (ground_locg.py:467-478); m is Hermitian, row-major.
+__device__ void eig2(const double2 m[2][2], double* val, double2 vec[2]) {
+  const double d0 = m[0][0].x, d1 = m[1][1].x;
+  const double det = d0 * d1 - cabs2(m[1][0]);
+  const double tr = d0 + d1;
+  const double ev = (tr - sqrt(tr * tr - 4.0 * det)) * 0.5;
+  const double2 num = make_double2(d1 - ev + m[1][0].x, -m[1][0].y);
+  const double2 den = make_double2(d0 - ev + m[1][0].x, m[1][0].y);
+  double2 v0 = cdiv(num, den);
+  const double nrm = sqrt(v0.x * v0.x + v0.y * v0.y + 1.0);
+  vec[0] = cscale(v0, 1.0 / nrm);
+  vec[1] = make_double2(-1.0 / nrm, 0.0);
+  *val = ev;
+}
+
+// eigenpair_3x3 (ground_locg.py:481-514): Cardano's method after J. Kopp, Int. J. Mod. Phys. C
+// 19, 523 (2008), lowest eigenvalue, eigenvector from the cross product of two columns of
+// (m - lambda).
+__device__ void eig3(const double2 m[3][3], double* val, double2 vec[3]) {
+  const double d0 = m[0][0].x, d1 = m[1][1].x, d2 = m[2][2].x;
+  const double mo0 = cabs2(m[1][0]), mo1 = cabs2(m[2][0]), mo2 = cabs2(m[2][1]);
+  const double c2 = -(d0 + d1 + d2);
+  const double c1 = (d0 * d2 + d1 * d0 + d2 * d1) - (mo0 + mo1 + mo2);
+  double c0 = d0 * mo2 + d1 * mo1 + d2 * mo0;
+  c0 -= d0 * d1 * d2;
+  c0 -= 2.0 * cmul(cmul(m[0][2], m[1][0]), m[2][1]).x;
+  const double p = c2 * c2 - 3.0 * c1;
+  const double q = -13.5 * c0 - c2 * c2 * c2 + 4.5 * c2 * c1;
+  const double phi =
+      atan2(sqrt(27.0 * (0.25 * c1 * c1 * (p - c1) + c0 * (q + 6.75 * c0))), q) / 3.0;
+  const double cphi = cos(phi), sphi = sin(phi);
+  const double s3 = sqrt(3.0);
+  const double xmin = fmin(fmin(2.0 * cphi, -cphi - s3 * sphi), -cphi + s3 * sphi);
+  const double ev = sqrt(p) / 3.0 * xmin - c2 / 3.0;
+  double2 a[3] = {m[0][1], m[1][1], m[2][1]};
+  double2 b[3] = {m[0][2], m[1][2], m[2][2]};
+  a[1].x -= ev;
+  b[2].x -= ev;
+  double2 cr[3];
+  cr[0] = cconj(csub(cmul(a[1], b[2]), cmul(a[2], b[1])));
+  cr[1] = cconj(csub(cmul(a[2], b[0]), cmul(a[0], b[2])));
+  cr[2] = cconj(csub(cmul(a[0], b[1]), cmul(a[1], b[0])));
+  const double nrm = sqrt(cr[0].x * cr[0].x + cr[1].x * cr[1].x + cr[2].x * cr[2].x +
+                          cr[0].y * cr[0].y + cr[1].y * cr[1].y + cr[2].y * cr[2].y);
+  for (int k = 0; k < 3; ++k) vec[k] = cscale(cr[k], 1.0 / nrm);
+  *val = ev;
+}
+
+__device__ __forceinline__ double2 red_c(const LocgDev* d, int k) {
+  return make_double2(d->red[k][0], d->red[k][1]);
+}
+__device__ __forceinline__ void set_coef(LocgDev* d, int o, int k, double2 c) {
+  d->coef[o][k][0] = c.x;
+  d->coef[o][k][1] = c.y;
+}
+__device__ __forceinline__ void set_coef_r(LocgDev* d, int o, int k, double c) {
+  d->coef[o][k][0] = c;
+  d->coef[o][k][1] = 0.0;
+}
+
+__device__ void run_post(LocgDev* d, int post, int nsrc, int use_cond,
+                         cudaGraphConditionalHandle cond) {
+  switch (post) {
+    case P_NONE: break;
+    case P_INV_NORM: set_coef_r(d, 0, 0, 1.0 / sqrt(d->red[0][0])); break;
+    case P_THETA0: {
+      d->theta = d->red[0][0];
+      set_coef_r(d, 0, 0, 1.0);
+      set_coef_r(d, 0, 1, -d->theta);
+    } break;
+    case P_R0NORM: {
+      d->rnorm = sqrt(d->red[0][0]);
+      d->rzero = d->rnorm == 0.0;
+      set_coef_r(d, 0, 0, 1.0 / d->rnorm);
+    } break;
+    case P_RR2: {
+      double2 m[2][2];
+      m[0][0] = red_c(d, 0);
+      m[1][0] = red_c(d, 1);
+      m[0][1] = cconj(m[1][0]);
+      m[1][1] = red_c(d, 2);
+      double ev;
+      double2 k[2];
+      eig2(m, &ev, k);
+      d->theta = ev;
+      // t = p k0 - x k1 ; u = x k0 + p k1   (sources x, p)
+      set_coef(d, 0, 0, make_double2(-k[1].x, -k[1].y));
+      set_coef(d, 0, 1, k[0]);
+      set_coef(d, 1, 0, k[0]);
+      set_coef(d, 1, 1, k[1]);
+    } break;
+    case P_TU_NORM: {
+      // red0 = |t|^2, red1 = |u|^2 ; sources (u, t): x = u/|u|, y = t/|t|
+      set_coef_r(d, 0, 0, 1.0 / sqrt(d->red[1][0]));
+      set_coef_r(d, 0, 1, 0.0);
+      set_coef_r(d, 1, 0, 0.0);
+      set_coef_r(d, 1, 1, 1.0 / sqrt(d->red[0][0]));
+    } break;
+    case P_PROJ_IPS: {
+      set_coef_r(d, 0, 0, 1.0);
+      set_coef(d, 0, 1, make_double2(-d->red[0][0], -d->red[0][1]));
+      set_coef(d, 0, 2, make_double2(-d->red[1][0], -d->red[1][1]));
+    } break;
+    case P_PROJ_NORM_IPS: {
+      const double nv = sqrt(d->red[0][0]);
+      const double s = nv == 0.0 ? 1.0 : 1.0 / nv;
+      set_coef_r(d, 0, 0, s);
+      set_coef(d, 0, 1, make_double2(-s * d->red[1][0], -s * d->red[1][1]));
+      set_coef(d, 0, 2, make_double2(-s * d->red[2][0], -s * d->red[2][1]));
+    } break;
+    case P_PROJ_MASK: {
+      d->keep = sqrt(d->red[0][0]) >= 0.99;
+      set_coef_r(d, 0, 0, d->keep ? 1.0 : 0.0);
+    } break;
+    case P_RR3: {
+      double2 m[3][3];
+      m[0][0] = red_c(d, 0);
+      m[1][1] = red_c(d, 1);
+      m[2][2] = red_c(d, 2);
+      m[1][0] = red_c(d, 3);
+      m[2][0] = red_c(d, 4);
+      m[2][1] = red_c(d, 5);
+      m[0][1] = cconj(m[1][0]);
+      m[0][2] = cconj(m[2][0]);
+      m[1][2] = cconj(m[2][1]);
+      double ev;
+      double2 k[3];
+      eig3(m, &ev, k);
+      d->theta_prev = d->theta;
+      d->theta = ev;
+      for (int i = 0; i < 3; ++i) {
+        d->kappa[i][0] = k[i].x;
+        d->kappa[i][1] = k[i].y;
+      }
+      set_coef_r(d, 0, 0, 0.0);
+      set_coef(d, 0, 1, k[1]);
+      set_coef(d, 0, 2, k[2]);
+    } break;
+    case P_SNORM: {
+      const double ns = sqrt(d->red[0][0]);
+      const double2 k0 = make_double2(d->kappa[0][0], d->kappa[0][1]);
+      const double2 k1 = make_double2(d->kappa[1][0], d->kappa[1][1]);
+      const double2 k2 = make_double2(d->kappa[2][0], d->kappa[2][1]);
+      // u = k0 x + k1 y + k2 p
+      set_coef(d, 0, 0, k0);
+      set_coef(d, 0, 1, k1);
+      set_coef(d, 0, 2, k2);
+      // t = (k0/ns)(k1 y + k2 p) - ns x
+      const double2 f = cscale(k0, 1.0 / ns);
+      set_coef_r(d, 1, 0, -ns);
+      set_coef(d, 1, 1, cmul(k1, f));
+      set_coef(d, 1, 2, cmul(k2, f));
+    } break;
+    case P_XY_NORM: {
+      set_coef_r(d, 0, 0, 1.0 / sqrt(d->red[0][0]));
+      set_coef_r(d, 0, 1, 0.0);
+      set_coef_r(d, 1, 0, 0.0);
+      set_coef_r(d, 1, 1, 1.0 / sqrt(d->red[1][0]));
+    } break;
+    case P_CONV:
+    case P_CONV_SPLIT: {
+      const double r = sqrt(d->red[0][0]);
+      const double ax2 = post == P_CONV ? d->red[1][0] : d->axnorm2;
+      d->rnorm = r;
+      d->niter += 1;
+      bool conv;
+      if (d->inner_rtol > 0.0) {
+        conv = r < d->inner_rtol * fabs(d->theta);
+        if (r < 0.5 * d->best_r) {
+          d->best_r = r;
+          d->best_it = d->niter;
+        }
+        if (d->stall > 0 && d->niter - d->best_it > d->stall) conv = true;
+      } else {
+        const double reltol = (sqrt(ax2) - d->theta) * d->nscale;
+        conv = r < d->tol * reltol;
+      }
+      if (d->etol > 0.0 && d->niter >= 2 &&
+          fabs(d->theta - d->theta_prev) <= d->etol * fabs(d->theta))
+        conv = true;
+      d->converged = conv;
+      d->done = conv || d->niter >= d->maxiter;
+      if (use_cond) cudaGraphSetConditional(cond, d->done ? 0u : 1u);
+    } break;
+    case P_STORE_AX: d->axnorm2 = d->red[0][0]; break;
+    case P_ORTH_IPS: {
+      set_coef_r(d, 0, 0, 1.0);
+      for (int k = 1; k < nsrc; ++k)
+        set_coef(d, 0, k, make_double2(-d->red[k - 1][0], -d->red[k - 1][1]));
+    } break;
+    case P_ORTH_NORM: {
+      const double nv = sqrt(d->red[0][0]);
+      set_coef_r(d, 0, 0, nv == 0.0 ? 1.0 : 1.0 / nv);
+    } break;
+    case P_SET_R_COEF: {
+      set_coef_r(d, 0, 0, 1.0);
+      set_coef_r(d, 0, 1, -d->theta);
+    } break;
+    case P_THETA_ONLY: d->theta = d->red[0][0]; break;
+    default: break;
+  }
+}
+
+// ----------------------------------------------------------------------------- fused pass
+template <typename R, int NC, int MAXS, int MAXD>
+__global__ void __launch_bounds__(LC_THREADS) k_lc(LCArgs<MAXS, MAXD> a) {
+  LocgDev* dev = a.dev;
+  if ((a.gate & G_DONE) && *(volatile int*)&dev->done) return;
+  if ((a.gate & G_KEEP) && *(volatile int*)&dev->keep) return;
+  double2 c[2][MAXS];
+#pragma unroll
+  for (int o = 0; o < 2; ++o)
+#pragma unroll
+    for (int k = 0; k < MAXS; ++k) c[o][k] = make_double2(dev->coef[o][k][0], dev->coef[o][k][1]);
+  double acc[MAXD][2];
+#pragma unroll
+  for (int d = 0; d < MAXD; ++d) acc[d][0] = acc[d][1] = 0.0;
+
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < a.n; i += stride) {
+    double2 s[MAXS];
+#pragma unroll
+    for (int k = 0; k < MAXS; ++k) {
+      if (k < a.nsrc) {
+        const Cx<R> v = ld_elem_rw<R, NC>(static_cast<const R*>(a.src[k]), i);
+        s[k] = make_double2(double(v.re), double(v.im));
+      } else {
+        s[k] = make_double2(0.0, 0.0);
+      }
+    }
+    double2 o[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      o[q] = make_double2(0.0, 0.0);
+      if (q < a.nout) {
+#pragma unroll
+        for (int k = 0; k < MAXS; ++k)
+          if (k < a.nsrc) o[q] = cadd(o[q], cmul(c[q][k], s[k]));
+        if constexpr (NC == 1) o[q].y = 0.0;
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < MAXD; ++d) {
+      if (d < a.ndot) {
+        double2 x = make_double2(0.0, 0.0), y = make_double2(0.0, 0.0);
+        const int ca = a.da[d], cb = a.db[d];
+#pragma unroll
+        for (int k = 0; k < MAXS; ++k) {
+          if (ca == k) x = s[k];
+          if (cb == k) y = s[k];
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          if (ca == 100 + q) x = o[q];
+          if (cb == 100 + q) y = o[q];
+        }
+        // conj(x) * y
+        acc[d][0] += x.x * y.x + x.y * y.y;
+        acc[d][1] += x.x * y.y - x.y * y.x;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+      if (q < a.nout && a.out[q] != nullptr)
+        st_elem<R, NC>(static_cast<R*>(a.out[q]), i, cx_make<R>(R(o[q].x), R(o[q].y)));
+  }
+
+  if (a.ndot == 0 && a.post == P_NONE) return;
+  // Block reduction of the dot accumulators.
+  __shared__ double sred[MAXD * 2][LC_THREADS / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 0; d < MAXD; ++d) {
+    if (d < a.ndot) {
+      const double v0 = warp_sum(acc[d][0]);
+      const double v1 = warp_sum(acc[d][1]);
+      if (lane == 0) {
+        sred[2 * d][warp] = v0;
+        sred[2 * d + 1][warp] = v1;
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * a.ndot) {
+    double t = 0.0;
+    for (int w = 0; w < LC_THREADS / 32; ++w) t += sred[threadIdx.x][w];
+    a.partials[static_cast<int64_t>(blockIdx.x) * (2 * MAXD) + threadIdx.x] = t;
+  }
+  __threadfence();
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(a.counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x < 2 * a.ndot) {
+    double t = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b)
+      t += *(volatile double*)&a.partials[static_cast<int64_t>(b) * (2 * MAXD) + threadIdx.x];
+    dev->red[threadIdx.x >> 1][threadIdx.x & 1] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    run_post(dev, a.post, a.nsrc, a.use_cond, a.cond);
+    *a.counter = 0u;
+  }
+}
+
+template <typename R, int NC>
+__global__ void k_onehot(R* x, int64_t n, int64_t idx) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    st_elem<R, NC>(x, i, cx_make<R>(R(i == idx ? 1 : 0), R(0)));
+}
+
+template <typename RO, typename RI, int NC>
+__global__ void k_convert(const RI* in, RO* out, int64_t n) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const Cx<RI> v = ld_elem_rw<RI, NC>(in, i);
+    st_elem<RO, NC>(out, i, cx_make<RO>(RO(v.re), RO(v.im)));
+  }
+}
+
+// ----------------------------------------------------------------------------- host driver
+struct Vec {
+  void* p = nullptr;
+};
+
+template <typename R, int NC>
+class Locg {
+ public:
+  using Small = LCArgs<6, 6>;
+  using Large = LCArgs<kMaxOrth + 1, kMaxOrth>;
+
+  Locg(int64_t n, sqd_matvec_fn fn, void* ctx, cudaStream_t st)
+      : n_(n), fn_(fn), ctx_(ctx), st_(st) {
+    for (auto* b : {&x_, &y_, &r_, &p_, &ax_, &ay_, &ap_, &t0_})
+      b->alloc(static_cast<size_t>(n) * NC, st);
+    blocks_ = static_cast<unsigned>(
+        std::max<int64_t>(1, std::min<int64_t>((n + LC_THREADS - 1) / LC_THREADS,
+                                               4 * num_sms())));
+    partials_.alloc(static_cast<size_t>(blocks_) * 2 * 16, st);
+    counter_.alloc(1, st);
+    dev_.alloc(1, st);
+    SQD_CUDA(cudaMemsetAsync(counter_.ptr, 0, sizeof(unsigned), st));
+    SQD_CUDA(cudaMemsetAsync(dev_.ptr, 0, sizeof(LocgDev), st));
+    SQD_CUDA(cudaMallocHost(reinterpret_cast<void**>(&host_), sizeof(LocgDev)));
+  }
+  ~Locg() {
+    if (host_) cudaFreeHost(host_);
+  }
+
+  R* x() { return x_.ptr; }
+  LocgDev* dev() { return dev_.ptr; }
+
+  void set_params(double tol, double nscale, int maxiter, double inner_rtol, double etol,
+                  int stall) {
+    LocgDev h{};
+    h.tol = tol;
+    h.nscale = nscale;
+    h.maxiter = maxiter;
+    h.inner_rtol = inner_rtol;
+    h.etol = etol;
+    h.stall = stall;
+    h.best_r = 1e300;
+    // Copy only the parameter block; counters are reset here too.
+    SQD_CUDA(cudaMemcpyAsync(dev_.ptr, &h, sizeof(LocgDev), cudaMemcpyHostToDevice, st_));
+    SQD_CUDA(cudaStreamSynchronize(st_));
+  }
+
+  // ---- one fused pass
+  void lc(std::initializer_list<const void*> srcs, std::initializer_list<void*> outs,
+          std::initializer_list<std::pair<int, int>> dots, int post, int gate = G_NONE) {
+    if (srcs.size() <= 6 && dots.size() <= 6) {
+      Small a{};
+      fill(a, srcs, outs, dots, post, gate);
+      k_lc<R, NC, 6, 6><<<blocks_, LC_THREADS, 0, st_>>>(a);
+    } else {
+      Large a{};
+      fill(a, srcs, outs, dots, post, gate);
+      k_lc<R, NC, kMaxOrth + 1, kMaxOrth><<<blocks_, LC_THREADS, 0, st_>>>(a);
+    }
+    SQD_CHECK_LAUNCH();
+  }
+
+  // Runs only the scalar step `post` (one thread).
+  void post_only(int post, int gate = G_NONE) {
+    Small a{};
+    fill(a, {}, {}, {}, post, gate);
+    a.n = 0;
+    k_lc<R, NC, 6, 6><<<1, LC_THREADS, 0, st_>>>(a);
+    SQD_CHECK_LAUNCH();
+  }
+
+  void matvec(const void* in, void* out) {
+    const int rc = fn_(ctx_, in, out, st_);
+    if (rc != SQD_OK) throw Error(rc, std::string("matvec callback failed: ") + last_msg());
+  }
+
+  void read_host() {
+    SQD_CUDA(cudaMemcpyAsync(host_, dev_.ptr, sizeof(LocgDev), cudaMemcpyDeviceToHost, st_));
+    SQD_CUDA(cudaStreamSynchronize(st_));
+  }
+  const LocgDev& host() const { return *host_; }
+
+  // project_out(orth, v, normalize) with n_orth basis vectors (ground_locg.py:426-464).
+  void project_orth(const std::vector<const void*>& orth, void* v, bool normalize, int gate) {
+    if (orth.empty()) return;
+    for (int round = 0; round < 4; ++round) {
+      std::vector<std::pair<int, int>> dd;
+      for (size_t k = 0; k < orth.size(); ++k) dd.push_back({static_cast<int>(k + 1), 0});
+      lc_vec(orth, v, {}, dd, P_ORTH_IPS, gate);
+      const bool norm_now = normalize && round < 2;
+      lc_vec(orth, v, {v}, norm_now ? std::vector<std::pair<int, int>>{{100, 100}}
+                                     : std::vector<std::pair<int, int>>{},
+             norm_now ? P_ORTH_NORM : P_NONE, gate);
+      if (norm_now) lc({v}, {v}, {}, P_NONE, gate);
+    }
+    if (normalize) {
+      lc({v}, {}, {{0, 0}}, P_PROJ_MASK, gate);
+      lc({v}, {v}, {}, P_NONE, gate | G_KEEP);
+    }
+  }
+
+  // ---------------------------------------------------------------- the faithful algorithm
+  // Start: x already holds xinit (unnormalised).  Returns after iter0 and iter1.
+  void start(const std::vector<const void*>& orth) {
+    R* x = x_.ptr;
+    lc({x}, {}, {{0, 0}}, P_INV_NORM);
+    lc({x}, {x}, {}, P_NONE);
+    // body_iter0 (:280-291)
+    matvec(x, ax_.ptr);
+    project_orth(orth, ax_.ptr, false, G_NONE);
+    lc({ax_.ptr, x}, {}, {{1, 0}}, P_THETA0);
+    lc({ax_.ptr, x}, {r_.ptr}, {{100, 100}}, P_R0NORM);
+    read_host();
+    if (host_->rzero) {
+      SQD_CUDA(cudaMemsetAsync(y_.ptr, 0, sizeof(R) * NC * n_, st_));
+      return;
+    }
+    // body_iter1 (:293-322)
+    lc({r_.ptr}, {p_.ptr}, {}, P_NONE);
+    matvec(x, ax_.ptr);
+    matvec(p_.ptr, ap_.ptr);
+    lc({x, p_.ptr, ax_.ptr, ap_.ptr}, {}, {{0, 2}, {1, 2}, {1, 3}}, P_RR2);
+    lc({x, p_.ptr}, {t0_.ptr, ay_.ptr}, {{100, 100}, {101, 101}}, P_TU_NORM);  // t, u
+    lc({ay_.ptr, t0_.ptr}, {x, y_.ptr}, {}, P_NONE);
+    project_orth(orth, x, true, G_NONE);
+    matvec(x, ax_.ptr);
+    post_only(P_SET_R_COEF);
+    lc({ax_.ptr, x}, {r_.ptr}, {}, P_NONE);
+    project_orth(orth, r_.ptr, false, G_NONE);
+  }
+
+  // One body iteration (:324-383).  All passes are gated on `done`.
+  void body(const std::vector<const void*>& orth) {
+    R *x = x_.ptr, *y = y_.ptr, *r = r_.ptr, *p = p_.ptr;
+    const int g = G_DONE;
+    // p = project_out((x, y), r): 4 rounds, normalising in the first two.
+    lc({r, x, y}, {}, {{1, 0}, {2, 0}}, P_PROJ_IPS, g);
+    lc({r, x, y}, {p}, {{100, 100}, {1, 100}, {2, 100}}, P_PROJ_NORM_IPS, g);
+    lc({p, x, y}, {p}, {{100, 100}, {1, 100}, {2, 100}}, P_PROJ_NORM_IPS, g);
+    lc({p, x, y}, {p}, {{1, 100}, {2, 100}}, P_PROJ_IPS, g);
+    lc({p, x, y}, {p}, {{100, 100}}, P_PROJ_MASK, g);
+    lc({p}, {p}, {}, P_NONE, g | G_KEEP);
+    // Rayleigh-Ritz on {x, y, p}
+    matvec(x, ax_.ptr);
+    matvec(y, ay_.ptr);
+    matvec(p, ap_.ptr);
+    lc({x, y, p, ax_.ptr, ay_.ptr, ap_.ptr}, {}, {{0, 3}, {1, 4}, {2, 5}, {1, 3}, {2, 3}, {2, 4}},
+       P_RR3, g);
+    // s = k1 y + k2 p (virtual), |s|
+    lc({x, y, p}, {nullptr}, {{100, 100}}, P_SNORM, g);
+    // u -> x, t -> y (in place), norms
+    lc({x, y, p}, {x, y}, {{100, 100}, {101, 101}}, P_XY_NORM, g);
+    lc({x, y}, {x, y}, {}, orth.empty() ? P_SET_R_COEF : P_NONE, g);
+    project_orth(orth, x, true, g);
+    matvec(x, ax_.ptr);
+    if (!orth.empty()) post_only(P_SET_R_COEF, g);
+    if (orth.empty()) {
+      lc({ax_.ptr, x}, {r}, {{100, 100}, {0, 0}}, P_CONV, g);
+    } else {
+      lc({ax_.ptr, x}, {r}, {{0, 0}}, P_STORE_AX, g);
+      project_orth(orth, r, false, g);
+      lc({r}, {}, {{0, 0}}, P_CONV_SPLIT, g);
+    }
+  }
+
+  // Runs the while-loop.  use_graph: one CUDA graph with a conditional WHILE node.
+  void loop(const std::vector<const void*>& orth, int maxiter, bool use_graph) {
+    read_host();
+    if (maxiter <= 0) return;
+    if (!use_graph) {
+      for (;;) {
+        body(orth);
+        read_host();
+        if (host_->done) break;
+      }
+      return;
+    }
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    SQD_CUDA(cudaGraphCreate(&graph, 0));
+    try {
+      SQD_CUDA(cudaGraphConditionalHandleCreate(&cond_, graph, 1, cudaGraphCondAssignDefault));
+      cudaGraphNodeParams cp{};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = cond_;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t node;
+      SQD_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+      cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+      use_cond_ = 1;
+      SQD_CUDA(cudaStreamBeginCaptureToGraph(st_, bodyg, nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeThreadLocal));
+      try {
+        body(orth);
+      } catch (...) {
+        cudaGraph_t dummy;
+        cudaStreamEndCapture(st_, &dummy);
+        use_cond_ = 0;
+        throw;
+      }
+      SQD_CUDA(cudaStreamEndCapture(st_, &bodyg));
+      use_cond_ = 0;
+      SQD_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+      SQD_CUDA(cudaGraphLaunch(exec, st_));
+      read_host();
+    } catch (...) {
+      if (exec) cudaGraphExecDestroy(exec);
+      cudaGraphDestroy(graph);
+      throw;
+    }
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+  }
+
+  DevBuf<R> x_, y_, r_, p_, ax_, ay_, ap_, t0_;
+
+ private:
+  template <typename A>
+  void fill(A& a, std::initializer_list<const void*> srcs, std::initializer_list<void*> outs,
+            std::initializer_list<std::pair<int, int>> dots, int post, int gate) {
+    a.n = n_;
+    int k = 0;
+    for (auto s : srcs) a.src[k++] = s;
+    a.nsrc = k;
+    k = 0;
+    for (auto o : outs) a.out[k++] = o;
+    a.nout = k;
+    k = 0;
+    for (auto d : dots) {
+      a.da[k] = static_cast<signed char>(d.first);
+      a.db[k] = static_cast<signed char>(d.second);
+      ++k;
+    }
+    a.ndot = k;
+    a.post = post;
+    a.gate = gate;
+    a.dev = dev_.ptr;
+    a.partials = partials_.ptr;
+    a.counter = counter_.ptr;
+    a.use_cond = use_cond_;
+    a.cond = cond_;
+  }
+  // Variant for the orth projection: sources (v, o_0, ..., o_{m-1}).
+  void lc_vec(const std::vector<const void*>& orth, void* v, std::vector<void*> outs,
+              const std::vector<std::pair<int, int>>& dots, int post, int gate) {
+    Large a{};
+    a.n = n_;
+    a.src[0] = v;
+    for (size_t k = 0; k < orth.size(); ++k) a.src[k + 1] = orth[k];
+    a.nsrc = static_cast<int>(orth.size() + 1);
+    a.nout = static_cast<int>(outs.size());
+    for (size_t k = 0; k < outs.size(); ++k) a.out[k] = outs[k];
+    a.ndot = static_cast<int>(dots.size());
+    for (size_t k = 0; k < dots.size(); ++k) {
+      a.da[k] = static_cast<signed char>(dots[k].first);
+      a.db[k] = static_cast<signed char>(dots[k].second);
+    }
+    a.post = post;
+    a.gate = gate;
+    a.dev = dev_.ptr;
+    a.partials = partials_.ptr;
+    a.counter = counter_.ptr;
+    a.use_cond = use_cond_;
+    a.cond = cond_;
+    k_lc<R, NC, kMaxOrth + 1, kMaxOrth><<<blocks_, LC_THREADS, 0, st_>>>(a);
+    SQD_CHECK_LAUNCH();
+  }
+  static std::string last_msg() {
+    const char* m = sqd_last_error();
+    return m ? m : "";
+  }
+
+  int64_t n_;
+  sqd_matvec_fn fn_;
+  void* ctx_;
+  cudaStream_t st_;
+  unsigned blocks_ = 1;
+  DevBuf<double> partials_;
+  DevBuf<unsigned> counter_;
+  DevBuf<LocgDev> dev_;
+  LocgDev* host_ = nullptr;
+  int use_cond_ = 0;
+  cudaGraphConditionalHandle cond_ = 0;
+};
+
+// Matvec adapter for the FP32 phase of the mixed solver.
+struct OpCtx32 {
+  sqd_op_s* op;
+  int dtype;
+};
+int op_cb32(void* ctx, const void* x, void* y, void* stream) {
+  auto* c = static_cast<OpCtx32*>(ctx);
+  return guarded([&] { op_matvec(c->op, x, y, c->dtype, as_stream(stream)); });
+}
+struct OpCtx64 {
+  sqd_op_s* op;
+  int dtype;
+};
+int op_cb64(void* ctx, const void* x, void* y, void* stream) {
+  auto* c = static_cast<OpCtx64*>(ctx);
+  return guarded([&] { op_matvec(c->op, x, y, c->dtype, as_stream(stream)); });
+}
+
+template <int NC>
+void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xinit,
+              int64_t xinit_index, const std::vector<const void*>& orth, double tol,
+              int maxiter, int mode, bool use_graph, cudaStream_t st, double* eigval,
+              void* eigvec, int* niter, double* residual) {
+  const double eps64 = 2.220446049250313e-16;
+  const double nscale = 10.0 * static_cast<double>(n);
+  const unsigned G = grid_for(n, 256, 8192);
+  if (mode == SQD_LOCG_FP64) {
+    Locg<double, NC> L(n, fn, ctx, st);
+    L.set_params(tol < 0 ? eps64 : tol, nscale, maxiter, 0.0, 0.0, 0);
+    if (xinit)
+      SQD_CUDA(cudaMemcpyAsync(L.x(), xinit, sizeof(double) * NC * n, cudaMemcpyDeviceToDevice,
+                               st));
+    else
+      k_onehot<double, NC><<<G, 256, 0, st>>>(L.x(), n, xinit_index);
+    SQD_CHECK_LAUNCH();
+    if (!xinit) L.project_orth(orth, L.x(), true, G_NONE);
+    L.start(orth);
+    L.loop(orth, maxiter, use_graph);
+    const LocgDev& h = L.host();
+    *eigval = h.theta;
+    *niter = h.niter;
+    if (residual) *residual = h.rnorm;
+    SQD_CUDA(cudaMemcpyAsync(eigvec, L.x(), sizeof(double) * NC * n, cudaMemcpyDeviceToDevice,
+                             st));
+    SQD_CUDA(cudaStreamSynchronize(st));
+    return;
+  }
+  // Mixed precision: FP32 sweeps (c64/f32 vectors, compensated FP32 matvec, FP64 reductions)
+  // until the FP32 residual stalls, then FP64 LOCG iterations from that vector (FP64 residual
+  // and Rayleigh-Ritz) until the reference's residual test holds or the Ritz value is stable.
+  SQD_REQUIRE(fn == sqd_op_matvec_cb, "mixed precision needs an sqd operator as the matvec");
+  auto* op = static_cast<sqd_op_s*>(ctx);
+  op_ensure_values32(op, st);
+  OpCtx32 c32{op, NC == 2 ? SQD_C64 : SQD_F32};
+  OpCtx64 c64{op, NC == 2 ? SQD_C128 : SQD_F64};
+  int it32 = 0;
+  DevBuf<double> x64;
+  x64.alloc(static_cast<size_t>(n) * NC, st);
+  {
+    Locg<float, NC> L(n, op_cb32, &c32, st);
+    L.set_params(0.0, nscale, maxiter, 2e-6, 0.0, 40);
+    if (xinit) {
+      k_convert<float, double, NC><<<G, 256, 0, st>>>(static_cast<const double*>(xinit), L.x(),
+                                                     n);
+    } else {
+      k_onehot<float, NC><<<G, 256, 0, st>>>(L.x(), n, xinit_index);
+    }
+    SQD_CHECK_LAUNCH();
+    L.start(orth);
+    L.loop(orth, maxiter, use_graph);
+    it32 = L.host().niter;
+    k_convert<double, float, NC><<<G, 256, 0, st>>>(L.x(), x64.ptr, n);
+    SQD_CHECK_LAUNCH();
+  }
+  Locg<double, NC> L(n, op_cb64, &c64, st);
+  L.set_params(tol < 0 ? eps64 : tol, nscale, std::max(1, maxiter - it32), 0.0, 1e-13, 0);
+  SQD_CUDA(cudaMemcpyAsync(L.x(), x64.ptr, sizeof(double) * NC * n, cudaMemcpyDeviceToDevice,
+                           st));
+  L.start(orth);
+  L.loop(orth, std::max(1, maxiter - it32), use_graph);
+  const LocgDev& h = L.host();
+  *eigval = h.theta;
+  *niter = it32 + h.niter;
+  if (residual) *residual = h.rnorm;
+  SQD_CUDA(cudaMemcpyAsync(eigvec, L.x(), sizeof(double) * NC * n, cudaMemcpyDeviceToDevice,
+                           st));
+  SQD_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace
+}  // namespace sqd
+
+using namespace sqd;
+
+extern "C" int sqd_op_matvec_cb(void* ctx, const void* x, void* y, void* stream) {
+  return guarded([&] {
+    SQD_REQUIRE(ctx != nullptr, "NULL operator");
+    auto* op = static_cast<sqd_op_s*>(ctx);
+    // Applies the operator to complex128 vectors (sqd_locg substitutes its own dtype).
+    op_matvec(op, x, y, SQD_C128, as_stream(stream));
+  });
+}
+
+// Operator callback with an explicit dtype (used by the FP64 solver).
+namespace {
+struct OpDtypeCtx {
+  sqd_op_s* op;
+  int dtype;
+};
+int op_dtype_cb(void* ctx, const void* x, void* y, void* stream) {
+  auto* c = static_cast<OpDtypeCtx*>(ctx);
+  return guarded([&] { op_matvec(c->op, x, y, c->dtype, as_stream(stream)); });
+}
+}  // namespace
+
+extern "C" int sqd_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xinit,
+                        int64_t xinit_index, const void* const* orth, int n_orth, double tol,
+                        int maxiter, int mode, int use_graph, void* stream, double* eigval_host,
+                        void* eigvec, int* niter_host, double* residual_host) {
+  return guarded([&] {
+    SQD_REQUIRE(n >= 1, "empty vector space");
+    SQD_REQUIRE(dtype == SQD_F64 || dtype == SQD_C128, "LOCG result dtype must be F64 or C128");
+    SQD_REQUIRE(fn != nullptr, "NULL matvec");
+    SQD_REQUIRE(eigval_host && eigvec && niter_host, "NULL output");
+    SQD_REQUIRE(n_orth >= 0 && n_orth <= kMaxOrth, "at most 8 orth vectors");
+    SQD_REQUIRE(mode == SQD_LOCG_FP64 || mode == SQD_LOCG_MIXED, "bad LOCG mode");
+    SQD_REQUIRE(xinit != nullptr || (xinit_index >= 0 && xinit_index < n),
+                "xinit index out of range");
+    cudaStream_t st = as_stream(stream);
+    std::vector<const void*> ov;
+    for (int k = 0; k < n_orth; ++k) ov.push_back(orth[k]);
+    SQD_REQUIRE(mode == SQD_LOCG_FP64 || ov.empty(), "mixed precision does not support orth");
+    OpDtypeCtx octx{nullptr, dtype};
+    sqd_matvec_fn f = fn;
+    void* c = ctx;
+    bool graph = use_graph != 0;
+    if (fn == sqd_op_matvec_cb) {
+      octx.op = static_cast<sqd_op_s*>(ctx);
+      SQD_REQUIRE(octx.op->s->states_size == n, "vector size differs from the operator size");
+      SQD_REQUIRE(dtype == SQD_C128 || !octx.op->value_complex,
+                  "a complex Hamiltonian needs complex vectors");
+      if (mode == SQD_LOCG_FP64) {
+        f = op_dtype_cb;
+        c = &octx;
+      }
+    } else {
+      graph = false;  // foreign callbacks may synchronise; no capture
+    }
+    if (dtype == SQD_C128)
+      run_locg<2>(n, dtype, f, c, xinit, xinit_index, ov, tol, maxiter, mode, graph, st,
+                  eigval_host, eigvec, niter_host, residual_host);
+    else
+      run_locg<1>(n, dtype, f, c, xinit, xinit_index, ov, tol, maxiter, mode, graph, st,
+                  eigval_host, eigvec, niter_host, residual_host);
+  });
+}
