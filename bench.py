@@ -1,0 +1,395 @@
+"""Benchmark of the SQD hot path on B200.
+
+Default workload (one GPU): the 32-qubit Jordan-Wigner molecular Hamiltonian (16 spatial
+orbitals, h1 ~ N(0,1)/16, h2 ~ N(0,0.1) with 8-fold symmetry, seed 0) on the 512 x 512
+alpha/beta product subspace of 4-electron strings (D = 262,144), complex128 vectors.
+
+A step is one Pauli-sum matvec Hv over the whole subspace (the inner kernel of LOCG).  ``value``
+is row.terms/s = (rows x merged terms) / step time, summed over ranks (replicas, weak scaling),
+with inputs resident in HBM; ``e2e`` is the same metric through the public API with the input
+vector copied from pinned host memory and the result copied back inside the timed region.
+Beside it: the roofline of the matvec kernel, the LOCG time-to-E0 (FP64 and mixed precision),
+and the CPU baseline (the reference's default matvec algorithm on the host cores, on a row
+sample).  ``--impl reference`` times only that CPU path.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                       [--workload c2|c1|c3|c5] [--cache 1,0|1,2|0,0] [--no-locg]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'matvec row.terms/s (SQD Pauli-sum matvec over the sampled subspace)'
+UNIT = 'row.terms/s'
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--workload', default='c2', choices=['c1', 'c2', 'c3', 'c5'])
+    ap.add_argument('--cache', default='1,2')
+    ap.add_argument('--no-locg', action='store_true')
+    ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--cpu-rows', type=int, default=0, help='CPU sample rows (0 = auto)')
+    ap.add_argument('--lanes', type=int, default=0, help='lanes per row (0 = autotune)')
+    return ap.parse_args()
+
+
+def make_workload(name):
+    from rqutils_b200 import workloads as W
+    return {'c1': W.c1, 'c2': W.c2, 'c3': W.c3, 'c5': W.c5}[name](0)
+
+
+def workload_config(wl, cache):
+    cfg = {'workload': f'{wl.name}: {wl.num_qubits}-qubit '
+                       + ('JW molecular Hamiltonian, alpha x beta product subspace'
+                          if wl.name in ('c2', 'c3') else 'random Pauli sum, weight subspace'),
+           'num_qubits': wl.num_qubits, 'subspace_dim': int(wl.states.shape[0]),
+           'raw_terms': int(wl.coeffs.shape[0]), 'seed': wl.seed,
+           'cache_strategy': list(cache), 'vector_dtype': 'complex128',
+           'l2': 'no flush: stored pairs read per step exceed the 126 MB L2'}
+    cfg.update({k: v for k, v in wl.notes.items() if k in ('norb', 'nelec', 'na', 'nb')})
+    return cfg
+
+
+def load_peaks():
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d['hbm_gbs']), 'measured'
+    return 6650.0, 'fallback'
+
+
+def load_traffic(workload, cache):
+    """DRAM traffic per launch of the matvec kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, 'profiles', f'matvec_{workload}_cache{cache[0]}{cache[1]}.md')
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith('traffic_bytes_per_launch:'):
+            return float(line.split(':', 1)[1])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', f'--id={self.index}', f'--query-gpu={self.QUERY}',
+                 '--format=csv,noheader,nounits', '-lms', '100'],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == 'active':
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': max(mx),
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def init_dist(n_gpus):
+    import torch
+    import torch.distributed as dist
+    if n_gpus <= 1 or 'RANK' not in os.environ:
+        return 0, 1, None
+    from datetime import timedelta
+    local = int(os.environ.get('LOCAL_RANK', 0))
+    torch.cuda.set_device(local)
+    dist.init_process_group('nccl', timeout=timedelta(seconds=120),
+                            device_id=torch.device('cuda', local))
+    return dist.get_rank(), dist.get_world_size(), dist
+
+
+def max_over_ranks(val, dist, device='cuda'):
+    """Slowest rank's time: every rank takes part in the same collective."""
+    if dist is None:
+        return val
+    import torch
+    t = torch.tensor([val], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(val, dist, device='cuda'):
+    """Whole-job total of per-rank work units."""
+    if dist is None:
+        return val
+    import torch
+    t = torch.tensor([val], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def replica_throughput(units_per_step, steps, t_local, dist, device='cuda'):
+    """value = units all ranks processed / max-over-ranks time (replicas, weak scaling)."""
+    t_max = max_over_ranks(t_local, dist, device)
+    return sum_over_ranks(units_per_step * steps, dist, device) / t_max, t_max
+
+
+def barrier(dist):
+    import torch
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+
+
+def cpu_baseline(wl, budget_s=20.0, rows=0):
+    """The reference's default matvec on the host cores over a bounded row sample."""
+    from oracle.cpu_baseline import CpuMatvecSample
+    n = wl.states.shape[0]
+    rng = np.random.default_rng(1)
+    if rows <= 0:
+        rows = min(n, 16384)
+    sample = np.sort(rng.choice(n, size=min(rows, n), replace=False))
+    cpu = CpuMatvecSample(wl.x, wl.z, wl.coeffs, wl.states, sample)
+    v = wl.start_vector(np.complex128)
+    t1 = cpu.time(v, reps=1)
+    # grow the sample to fill about budget_s of CPU work
+    if rows < n and t1 < budget_s / 4:
+        scale = min(n / rows, max(1.0, budget_s / 2 / max(t1, 1e-3)))
+        new_rows = int(min(n, rows * scale))
+        cpu.close()
+        sample = np.sort(rng.choice(n, size=new_rows, replace=False))
+        cpu = CpuMatvecSample(wl.x, wl.z, wl.coeffs, wl.states, sample)
+        t1 = cpu.time(v, reps=1)
+    m = cpu.num_terms
+    cpu.close()
+    val = sample.shape[0] * m / t1
+    return {'value': val, 'unit': UNIT, 'cores': cpu.nproc, 'kind': 'port',
+            'sample': f'{sample.shape[0]} of {n} rows, all {m} merged terms, one matvec '
+                      f'({t1:.1f} s), NumPy restatement of apply_h_x_cached + get_diagonal '
+                      f'over a spawn process pool'}
+
+
+def run_reference(args):
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return
+    wl = make_workload(args.workload)
+    from oracle.cpu_baseline import CpuMatvecSample
+    n = wl.states.shape[0]
+    rng = np.random.default_rng(1)
+    rows = args.cpu_rows or min(n, 16384)
+    sample = np.sort(rng.choice(n, size=rows, replace=False))
+    cpu = CpuMatvecSample(wl.x, wl.z, wl.coeffs, wl.states, sample)
+    v = wl.start_vector(np.complex128)
+    for _ in range(max(0, args.warmup)):
+        cpu.matvec(v)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cpu.matvec(v)
+    dt = (time.perf_counter() - t0) / max(1, args.steps)
+    cpu.close()
+    val = rows * cpu.num_terms / dt
+    sample_desc = (f'{rows} of {n} rows per step, all {cpu.num_terms} merged terms, NumPy '
+                   'restatement of apply_h_x_cached + get_diagonal (sqd.py:603-709) over a '
+                   'spawn process pool')
+    line = {'impl': 'reference', 'metric': METRIC, 'value': val, 'unit': UNIT,
+            'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': dt * 1e3, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'complex128', 'data': 'synthetic',
+            'config': workload_config(wl, (1, 0)),
+            'cpu_baseline': {'value': val, 'unit': UNIT, 'cores': cpu.nproc, 'kind': 'port',
+                             'sample': sample_desc},
+            'e2e': {'value': val, 'unit': UNIT, 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    rank, world, dist = init_dist(args.gpus)
+    if world == 1:
+        torch.cuda.set_device(0)
+    dev = torch.device('cuda', torch.cuda.current_device())
+    import rqutils_b200 as rq
+
+    cache = tuple(int(v) for v in args.cache.split(','))
+    wl = make_workload(args.workload)
+    ham = rq.PauliSumXZ.from_xz(wl.x, wl.z, wl.coeffs, wl.num_qubits, force_real=True,
+                                padded=True)
+    space = rq.Subspace.from_u64(wl.states, wl.num_qubits)
+    t_setup0 = time.perf_counter()
+    op = rq.SQDOperator(ham, space, cache_strategy=cache)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t_setup0
+    if args.lanes:
+        op.lanes_per_row = args.lanes
+        tuned = {'lanes_per_row': args.lanes, 'note': 'fixed by --lanes'}
+    else:
+        tuned = op.autotune(torch.complex128)
+    n_rows = space.states_size
+    m_terms = ham.num_terms
+    j_groups = ham.num_groups
+    nnz = op.nnz
+
+    v = torch.as_tensor(wl.start_vector(np.complex128), device=dev)
+    out = torch.empty_like(v)
+    stream = torch.cuda.current_stream()
+    for _ in range(max(3, args.warmup)):
+        op.matvec(v, out)
+    sampler = ClockSampler(dev.index) if rank == 0 else None
+    barrier(dist)
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    barrier(dist)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        op.matvec(v, out)
+    ev1.record(stream)
+    barrier(dist)
+    t_local = ev0.elapsed_time(ev1) / 1e3
+    units = n_rows * m_terms
+    value, t_max = replica_throughput(units, args.steps, t_local, dist)
+    gpu_launches = args.steps
+
+    # end to end: pinned host input -> device -> matvec -> pinned host output
+    v_host = v.cpu().pin_memory()
+    o_host = torch.empty_like(v_host).pin_memory()
+    v_dev = torch.empty_like(v)
+    for _ in range(3):
+        v_dev.copy_(v_host, non_blocking=True)
+        op.matvec(v_dev, out)
+        o_host.copy_(out, non_blocking=True)
+    barrier(dist)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        v_dev.copy_(v_host, non_blocking=True)
+        op.matvec(v_dev, out)
+        o_host.copy_(out, non_blocking=True)
+    e1.record(stream)
+    barrier(dist)
+    e2e_value, _ = replica_throughput(units, args.steps, e0.elapsed_time(e1) / 1e3, dist)
+    clocks = sampler.stop() if sampler else None
+    step_s = t_max / args.steps
+
+    # roofline of the matvec kernel (algorithmic bytes per launch)
+    w_v, w_c, W = 16, 16, 1
+    bytes_alg = n_rows * (8 * W + 2 * w_v) + nnz * w_v + m_terms * (8 * W + w_c) + j_groups * 8 * W
+    peak, peak_kind = load_peaks()
+    achieved = bytes_alg / (t_local / args.steps) / 1e9
+    traffic = load_traffic(args.workload, cache)
+
+    extra = {}
+    if not args.no_locg and rank == 0:
+        extra['locg'] = locg_times(rq, op, wl, dev)
+    line = None
+    if rank == 0:
+        line = {
+            'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': step_s * 1e3,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'complex128 (f64 arithmetic)', 'data': 'synthetic (seeded generator)',
+            'config': {**workload_config(wl, cache), 'parallelism': f'replicas x{world}',
+                       'merged_terms': m_terms, 'x_groups': j_groups, 'stored_pairs': nnz,
+                       'lanes_per_row': op.lanes_per_row, 'autotune': tuned,
+                       'setup_s': setup_s},
+            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                         'frac': achieved / peak, 'traffic': traffic,
+                         'peak_kind': peak_kind,
+                         'bytes_alg_per_launch': bytes_alg,
+                         'formula': 'N(8W+2w_v) + P_valid w_v + M(8W+w_c) + J 8W, W=1, '
+                                    'w_v=16, w_c=16, P_valid = stored pairs'},
+            'e2e': {'value': e2e_value, 'unit': UNIT,
+                    'h2d_bytes_per_step': int(v.numel() * 16),
+                    'd2h_bytes_per_step': int(v.numel() * 16)},
+            'gpu_launches': gpu_launches,
+            'clocks': clocks,
+        }
+        line.update(extra)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line['cpu_baseline'] = cpu_baseline(wl, rows=args.cpu_rows)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def locg_times(rq, op, wl, dev):
+    """Time-to-E0 of the FP64 path (reference algorithm) and of the mixed-precision path."""
+    import torch
+    x0 = torch.as_tensor(wl.start_vector(np.complex128), device=dev)
+    res = {'start_vector': 'complex128 N(0,1)+iN(0,1), normalised', 'tol': 1e-10}
+    for mode in ('fp64', 'mixed'):
+        rq.ground_locg(op, x0, tol=1e-10, maxiter=3, mode=mode)   # warm-up / graph build
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e, vec, it = rq.ground_locg(op, x0, tol=1e-10, mode=mode)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        res[mode] = {'time_to_e0_s': dt, 'eigval': e, 'niter': it,
+                     'residual': rq.ground_locg.last_residual}
+    e64 = res['fp64']['eigval']
+    res['mixed']['rel_err_vs_fp64'] = abs(res['mixed']['eigval'] - e64) / abs(e64)
+    res['speedup_mixed_vs_fp64'] = res['fp64']['time_to_e0_s'] / res['mixed']['time_to_e0_s']
+    return res
+
+
+def main():
+    args = parse()
+    if args.impl == 'reference':
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,57 @@
+"""Autotuner for the matvec schedule and lookup method.
+
+``tune_lanes`` times the cached matvec for every lanes-per-row choice (the number of warp
+lanes that share one output row) with CUDA events and keeps the fastest; ``tune_lookup``
+compares the hash-table and binary-search lookups on the connectivity build.  Results are
+cached per operator shape (rows, stored pairs, cache strategy, dtype) for the process.
+"""
+import torch
+
+_CACHE = {}
+
+
+def _time(fn, reps):
+    s = torch.cuda.current_stream()
+    fn()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(reps):
+        fn()
+    e1.record(s)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def tune_lanes(op, dtype, candidates=(2, 4, 8, 16, 32), reps=5):
+    if op.cache_strategy[0] != 1:
+        return {'lanes_per_row': None, 'note': 'uncached matvec has a fixed schedule'}
+    key = (op.size, op.nnz, op.cache_strategy, dtype)
+    if key in _CACHE:
+        op.lanes_per_row = _CACHE[key]['lanes_per_row']
+        return _CACHE[key]
+    v = torch.randn(op.size, dtype=dtype, device=op.space.device)
+    out = torch.empty_like(v)
+    times = {}
+    for lpr in candidates:
+        op.lanes_per_row = lpr
+        times[lpr] = _time(lambda: op.matvec(v, out), reps)
+    best = min(times, key=times.get)
+    op.lanes_per_row = best
+    res = {'lanes_per_row': best, 'ms': {str(k): round(t, 4) for k, t in times.items()}}
+    _CACHE[key] = res
+    return res
+
+
+def tune_lookup(hamiltonian, space, cache_strategy=(1, 0)):
+    """Builds the operator with each lookup method; returns (best, {method: seconds})."""
+    import time
+    from .sqd import SQDOperator
+    times = {}
+    for method in ('hash', 'bsearch'):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        SQDOperator(hamiltonian, space, cache_strategy, lookup=method)
+        torch.cuda.synchronize()
+        times[method] = time.perf_counter() - t0
+    return min(times, key=times.get), times

@@ -437,7 +437,7 @@ class Locg {
   using Large = LCArgs<kMaxOrth + 1, kMaxOrth>;
 
   Locg(int64_t n, sqd_matvec_fn fn, void* ctx, cudaStream_t st)
-      : n_(n), fn_(fn), ctx_(ctx), st_(st) {
+      : n_(n), fn_(fn), ctx_(ctx), st_(st), cur_(st) {
     for (auto* b : {&x_, &y_, &r_, &p_, &ax_, &ay_, &ap_, &t0_})
       b->alloc(static_cast<size_t>(n) * NC, st);
     blocks_ = static_cast<unsigned>(
@@ -478,11 +478,11 @@ class Locg {
     if (srcs.size() <= 6 && dots.size() <= 6) {
       Small a{};
       fill(a, srcs, outs, dots, post, gate);
-      k_lc<R, NC, 6, 6><<<blocks_, LC_THREADS, 0, st_>>>(a);
+      k_lc<R, NC, 6, 6><<<blocks_, LC_THREADS, 0, cur_>>>(a);
     } else {
       Large a{};
       fill(a, srcs, outs, dots, post, gate);
-      k_lc<R, NC, kMaxOrth + 1, kMaxOrth><<<blocks_, LC_THREADS, 0, st_>>>(a);
+      k_lc<R, NC, kMaxOrth + 1, kMaxOrth><<<blocks_, LC_THREADS, 0, cur_>>>(a);
     }
     SQD_CHECK_LAUNCH();
   }
@@ -492,12 +492,12 @@ class Locg {
     Small a{};
     fill(a, {}, {}, {}, post, gate);
     a.n = 0;
-    k_lc<R, NC, 6, 6><<<1, LC_THREADS, 0, st_>>>(a);
+    k_lc<R, NC, 6, 6><<<1, LC_THREADS, 0, cur_>>>(a);
     SQD_CHECK_LAUNCH();
   }
 
   void matvec(const void* in, void* out) {
-    const int rc = fn_(ctx_, in, out, st_);
+    const int rc = fn_(ctx_, in, out, cur_);
     if (rc != SQD_OK) throw Error(rc, std::string("matvec callback failed: ") + last_msg());
   }
 
@@ -616,18 +616,34 @@ class Locg {
       SQD_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
       cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
       use_cond_ = 1;
-      SQD_CUDA(cudaStreamBeginCaptureToGraph(st_, bodyg, nullptr, nullptr, 0,
-                                             cudaStreamCaptureModeThreadLocal));
+      // Capture on a private stream (the legacy default stream cannot be captured), launch on
+      // the caller's stream.
+      cudaStream_t cap = nullptr;
+      SQD_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+      cur_ = cap;
+      cudaError_t cerr = cudaStreamBeginCaptureToGraph(cap, bodyg, nullptr, nullptr, 0,
+                                                       cudaStreamCaptureModeThreadLocal);
+      if (cerr != cudaSuccess) {
+        cur_ = st_;
+        use_cond_ = 0;
+        cudaStreamDestroy(cap);
+        SQD_CUDA(cerr);
+      }
       try {
         body(orth);
       } catch (...) {
         cudaGraph_t dummy;
-        cudaStreamEndCapture(st_, &dummy);
+        cudaStreamEndCapture(cap, &dummy);
+        cur_ = st_;
         use_cond_ = 0;
+        cudaStreamDestroy(cap);
         throw;
       }
-      SQD_CUDA(cudaStreamEndCapture(st_, &bodyg));
+      cerr = cudaStreamEndCapture(cap, &bodyg);
+      cur_ = st_;
       use_cond_ = 0;
+      cudaStreamDestroy(cap);
+      SQD_CUDA(cerr);
       SQD_CUDA(cudaGraphInstantiate(&exec, graph, 0));
       SQD_CUDA(cudaGraphLaunch(exec, st_));
       read_host();
@@ -690,7 +706,7 @@ class Locg {
     a.counter = counter_.ptr;
     a.use_cond = use_cond_;
     a.cond = cond_;
-    k_lc<R, NC, kMaxOrth + 1, kMaxOrth><<<blocks_, LC_THREADS, 0, st_>>>(a);
+    k_lc<R, NC, kMaxOrth + 1, kMaxOrth><<<blocks_, LC_THREADS, 0, cur_>>>(a);
     SQD_CHECK_LAUNCH();
   }
   static std::string last_msg() {
@@ -702,6 +718,7 @@ class Locg {
   sqd_matvec_fn fn_;
   void* ctx_;
   cudaStream_t st_;
+  cudaStream_t cur_;  // launch stream: st_, or the private capture stream while capturing
   unsigned blocks_ = 1;
   DevBuf<double> partials_;
   DevBuf<unsigned> counter_;
