@@ -117,6 +117,15 @@ int sqd_diagonal(sqd_op_t op, int64_t group, void* out, int dtype, void* stream)
 /* vinit of run_sqd (sqd.py:406-426): argmin of the real group-0 diagonal over real rows when
  * group 0 has x = 0, else 0. */
 int sqd_vinit(sqd_op_t op, int64_t* index_host, void* stream);
+/* Same result as sqd_vinit, allocating nothing.  No counterpart in rqutils.  For callers that
+ * cannot allocate device memory when they pick the start vector (for example a process whose
+ * device memory is fully reserved by its own caching allocator or arena): the partial minima
+ * live in a fixed file-scope __device__ array (256 KiB, held by every GPU that loads the
+ * library until exit) instead of a per-call cudaMallocAsync.  Limit: 67,108,864 real rows,
+ * larger subspaces return SQD_ERR_INVALID.  The array is shared by all calls, so calls whose
+ * GPU work overlaps race; the first call on a device resolves the array's address and should
+ * come before any stream capture. */
+int sqd_vinit_noalloc(sqd_op_t op, int64_t* index_host, void* stream);
 /* Projected matrix <i|H|j> in CSR (hproj, sqd.py:269-314, with its padding bug fixed):
  * indptr[states_size+1] (int64), indices[nnz] (int32), data[nnz] complex128 (interleaved). */
 int sqd_op_csr(sqd_op_t op, int64_t* indptr, int32_t* indices, double* data, void* stream);

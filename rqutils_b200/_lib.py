@@ -62,6 +62,7 @@ PROTOTYPES = {
 EXTRA_PROTOTYPES = {
     'sqd_op_set_lanes': (_i32, [_vp, _i32]),
     'sqd_op_get_lanes': (_i32, [_vp, _c.POINTER(_i32)]),
+    'sqd_vinit_noalloc': (_i32, [_vp, _c.POINTER(_i64), _vp]),
 }
 
 
