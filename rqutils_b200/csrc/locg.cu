@@ -40,7 +40,9 @@ enum Post : int {
   P_ORTH_IPS,        // coef (1, -<o_k|v>...) over (v, o_0, ...)
   P_ORTH_NORM,       // s = 1/|v| (0 -> 1)
   P_SET_R_COEF,      // coef (1, -theta) for r = ax - theta x
-  P_THETA_ONLY       // theta = Re <x|ax> (refinement bookkeeping)
+  P_THETA_ONLY,      // theta = Re <x|ax> (refinement bookkeeping)
+  P_RESET,           // clear done/converged/stall tracking (restart of a loop)
+  P_CHECK0           // reference residual test on (|r|^2, |Ax|^2) without counting an iteration
 };
 
 struct LocgDev {
@@ -300,6 +302,19 @@ __device__ void run_post(LocgDev* d, int post, int nsrc, int use_cond,
       set_coef_r(d, 0, 1, -d->theta);
     } break;
     case P_THETA_ONLY: d->theta = d->red[0][0]; break;
+    case P_RESET: {
+      d->done = 0;
+      d->converged = 0;
+      d->best_r = 1e300;
+      d->best_it = d->niter;
+    } break;
+    case P_CHECK0: {
+      const double r = sqrt(d->red[0][0]);
+      d->rnorm = r;
+      const double reltol = (sqrt(d->red[1][0]) - d->theta) * d->nscale;
+      d->converged = r < d->tol * reltol;
+      d->done = d->converged;
+    } break;
     default: break;
   }
 }
@@ -590,13 +605,86 @@ class Locg {
     }
   }
 
-  // Runs the while-loop.  use_graph: one CUDA graph with a conditional WHILE node.
-  void loop(const std::vector<const void*>& orth, int maxiter, bool use_graph) {
+  // ------------------------------------------------------ implicit-product variant (FP32)
+  // Same Rayleigh-Ritz recurrence, but A x and A y are carried along as the same linear
+  // combinations as x and y, so an iteration needs one matvec (A p).  Used for the FP32
+  // sweeps of the mixed-precision solver; refresh() recomputes A x and A y to cancel drift.
+  void start_implicit() {
+    R* x = x_.ptr;
+    lc({x}, {}, {{0, 0}}, P_INV_NORM);
+    lc({x}, {x}, {}, P_NONE);
+    matvec(x, ax_.ptr);
+    lc({ax_.ptr, x}, {}, {{1, 0}}, P_THETA0);
+    lc({ax_.ptr, x}, {r_.ptr}, {{100, 100}}, P_R0NORM);
     read_host();
-    if (maxiter <= 0) return;
+    if (host_->rzero) {
+      SQD_CUDA(cudaMemsetAsync(y_.ptr, 0, sizeof(R) * NC * n_, st_));
+      SQD_CUDA(cudaMemsetAsync(ay_.ptr, 0, sizeof(R) * NC * n_, st_));
+      return;
+    }
+    lc({r_.ptr}, {p_.ptr}, {}, P_NONE);
+    matvec(p_.ptr, ap_.ptr);
+    lc({x, p_.ptr, ax_.ptr, ap_.ptr}, {}, {{0, 2}, {1, 2}, {1, 3}}, P_RR2);
+    lc({ax_.ptr, ap_.ptr}, {ay_.ptr, ax_.ptr}, {}, P_NONE);          // A t, A u
+    lc({x, p_.ptr}, {y_.ptr, x}, {{100, 100}, {101, 101}}, P_TU_NORM);  // t, u
+    lc({x, y_.ptr}, {x, y_.ptr}, {}, P_NONE);
+    lc({ax_.ptr, ay_.ptr}, {ax_.ptr, ay_.ptr}, {}, P_SET_R_COEF);
+    lc({ax_.ptr, x}, {r_.ptr}, {{100, 100}, {0, 0}}, P_CONV);
+  }
+
+  void body_implicit() {
+    R *x = x_.ptr, *y = y_.ptr, *r = r_.ptr, *p = p_.ptr;
+    R *ax = ax_.ptr, *ay = ay_.ptr, *ap = ap_.ptr;
+    const int g = G_DONE;
+    lc({r, x, y}, {}, {{1, 0}, {2, 0}}, P_PROJ_IPS, g);
+    lc({r, x, y}, {p}, {{100, 100}, {1, 100}, {2, 100}}, P_PROJ_NORM_IPS, g);
+    lc({p, x, y}, {p}, {{100, 100}, {1, 100}, {2, 100}}, P_PROJ_NORM_IPS, g);
+    lc({p, x, y}, {p}, {{1, 100}, {2, 100}}, P_PROJ_IPS, g);
+    lc({p, x, y}, {p}, {{100, 100}}, P_PROJ_MASK, g);
+    lc({p}, {p}, {}, P_NONE, g | G_KEEP);
+    matvec(p, ap);
+    lc({x, y, p, ax, ay, ap}, {}, {{0, 3}, {1, 4}, {2, 5}, {1, 3}, {2, 3}, {2, 4}}, P_RR3, g);
+    lc({x, y, p}, {nullptr}, {{100, 100}}, P_SNORM, g);
+    lc({ax, ay, ap}, {ax, ay}, {}, P_NONE, g);                      // A u, A t
+    lc({x, y, p}, {x, y}, {{100, 100}, {101, 101}}, P_XY_NORM, g);  // u, t
+    lc({x, y}, {x, y}, {}, P_NONE, g);
+    lc({ax, ay}, {ax, ay}, {}, P_SET_R_COEF, g);
+    lc({ax, x}, {r}, {{100, 100}, {0, 0}}, P_CONV, g);
+  }
+
+  // Recompute A x, A y and the residual explicitly; re-runs the convergence test.
+  void refresh() {
+    post_only(P_RESET);
+    matvec(x_.ptr, ax_.ptr);
+    matvec(y_.ptr, ay_.ptr);
+    lc({ax_.ptr, x_.ptr}, {}, {{1, 0}}, P_THETA0);
+    lc({ax_.ptr, x_.ptr}, {r_.ptr}, {{100, 100}, {0, 0}}, P_CONV);
+    read_host();
+  }
+
+  // Reference iteration 0 plus the reference residual test (no iteration counted).
+  void check0() {
+    R* x = x_.ptr;
+    lc({x}, {}, {{0, 0}}, P_INV_NORM);
+    lc({x}, {x}, {}, P_NONE);
+    matvec(x, ax_.ptr);
+    lc({ax_.ptr, x}, {}, {{1, 0}}, P_THETA0);
+    lc({ax_.ptr, x}, {r_.ptr}, {{100, 100}, {0, 0}}, P_CHECK0);
+    read_host();
+  }
+
+  // Runs the while-loop.  use_graph: one CUDA graph with a conditional WHILE node.
+  void loop(const std::vector<const void*>& orth, int maxiter, bool use_graph,
+            bool implicit = false) {
+    read_host();
+    if (maxiter <= 0 || host_->done) return;
+    auto run_body = [&] {
+      if (implicit) body_implicit();
+      else body(orth);
+    };
     if (!use_graph) {
       for (;;) {
-        body(orth);
+        run_body();
         read_host();
         if (host_->done) break;
       }
@@ -630,7 +718,7 @@ class Locg {
         SQD_CUDA(cerr);
       }
       try {
-        body(orth);
+        run_body();
       } catch (...) {
         cudaGraph_t dummy;
         cudaStreamEndCapture(cap, &dummy);
@@ -775,20 +863,28 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xin
     SQD_CUDA(cudaStreamSynchronize(st));
     return;
   }
-  // Mixed precision: FP32 sweeps (c64/f32 vectors, compensated FP32 matvec, FP64 reductions)
-  // until the FP32 residual stalls, then FP64 LOCG iterations from that vector (FP64 residual
-  // and Rayleigh-Ritz) until the reference's residual test holds or the Ritz value is stable.
+  // Mixed precision.
+  //  1. FP32 sweeps: complex64/f32 vectors, FP32 matrix elements with the compensated matvec,
+  //     FP64 inner products, implicit products (one matvec per iteration), until
+  //     |r| < kInnerRtol |theta| or the residual stops improving; A x and A y are then
+  //     recomputed explicitly and the test repeated (restarts cancel recurrence drift).
+  //  2. FP64 check: the vector is promoted, A x, theta and r are recomputed in FP64 and the
+  //     reference's residual test (ground_locg.py:371-376) is applied.
+  //  3. Only if it fails: FP64 iterations of the reference algorithm from that vector.
   SQD_REQUIRE(fn == sqd_op_matvec_cb, "mixed precision needs an sqd operator as the matvec");
   auto* op = static_cast<sqd_op_s*>(ctx);
   op_ensure_values32(op, st);
   OpCtx32 c32{op, NC == 2 ? SQD_C64 : SQD_F32};
   OpCtx64 c64{op, NC == 2 ? SQD_C128 : SQD_F64};
+  constexpr double kInnerRtol = 2e-7;
+  constexpr int kStall = 25;
+  constexpr int kRestarts = 6;
   int it32 = 0;
   DevBuf<double> x64;
   x64.alloc(static_cast<size_t>(n) * NC, st);
   {
     Locg<float, NC> L(n, op_cb32, &c32, st);
-    L.set_params(0.0, nscale, maxiter, 2e-6, 0.0, 40);
+    L.set_params(0.0, nscale, maxiter, kInnerRtol, 0.0, kStall);
     if (xinit) {
       k_convert<float, double, NC><<<G, 256, 0, st>>>(static_cast<const double*>(xinit), L.x(),
                                                      n);
@@ -796,21 +892,33 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xin
       k_onehot<float, NC><<<G, 256, 0, st>>>(L.x(), n, xinit_index);
     }
     SQD_CHECK_LAUNCH();
-    L.start(orth);
-    L.loop(orth, maxiter, use_graph);
+    L.start_implicit();
+    for (int k = 0; k < kRestarts; ++k) {
+      L.loop(orth, maxiter, use_graph, true);
+      if (L.host().niter >= maxiter || L.host().rzero) break;
+      L.refresh();
+      if (L.host().converged || L.host().niter >= maxiter) break;
+    }
     it32 = L.host().niter;
     k_convert<double, float, NC><<<G, 256, 0, st>>>(L.x(), x64.ptr, n);
     SQD_CHECK_LAUNCH();
   }
   Locg<double, NC> L(n, op_cb64, &c64, st);
-  L.set_params(tol < 0 ? eps64 : tol, nscale, std::max(1, maxiter - it32), 0.0, 1e-13, 0);
+  const int left = std::max(1, maxiter - it32);
+  L.set_params(tol < 0 ? eps64 : tol, nscale, left, 0.0, 0.0, 0);
   SQD_CUDA(cudaMemcpyAsync(L.x(), x64.ptr, sizeof(double) * NC * n, cudaMemcpyDeviceToDevice,
                            st));
-  L.start(orth);
-  L.loop(orth, std::max(1, maxiter - it32), use_graph);
+  L.check0();
+  int it64 = 0;
+  if (!L.host().converged) {
+    L.set_params(tol < 0 ? eps64 : tol, nscale, left, 0.0, 0.0, 0);
+    L.start(orth);
+    L.loop(orth, left, use_graph);
+    it64 = L.host().niter;
+  }
   const LocgDev& h = L.host();
   *eigval = h.theta;
-  *niter = it32 + h.niter;
+  *niter = it32 + it64;
   if (residual) *residual = h.rnorm;
   SQD_CUDA(cudaMemcpyAsync(eigvec, L.x(), sizeof(double) * NC * n, cudaMemcpyDeviceToDevice,
                            st));
