@@ -269,7 +269,7 @@ def run_ours(args):
         op.lanes_per_row = args.lanes
         tuned = {'lanes_per_row': args.lanes, 'note': 'fixed by --lanes'}
     else:
-        tuned = op.autotune(torch.complex128)
+        tuned = op.autotune()
     n_rows = space.states_size
     m_terms = ham.num_terms
     j_groups = ham.num_groups
@@ -339,7 +339,8 @@ def run_ours(args):
             'dtype': 'complex128 (f64 arithmetic)', 'data': 'synthetic (seeded generator)',
             'config': {**workload_config(wl, cache), 'parallelism': f'replicas x{world}',
                        'merged_terms': m_terms, 'x_groups': j_groups, 'stored_pairs': nnz,
-                       'lanes_per_row': op.lanes_per_row, 'autotune': tuned,
+                       'lanes_per_row': {'fp64': op.get_lanes(0), 'fp32': op.get_lanes(1)},
+                       'autotune': tuned,
                        'setup_s': setup_s},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                          'frac': achieved / peak, 'traffic': traffic,
@@ -369,16 +370,19 @@ def locg_times(rq, op, wl, dev):
     x0 = torch.as_tensor(wl.start_vector(np.complex128), device=dev)
     # tol=None: the reference default (dtype epsilon in its N-scaled test, ground_locg.py:
     # 224-225, 371-376), i.e. a converged FP64 energy to compare the mixed path against.
-    res = {'start_vector': 'complex128 N(0,1)+iN(0,1), normalised', 'tol': None}
+    res = {'start_vector': 'complex128 N(0,1)+iN(0,1), normalised', 'tol': None,
+           'timing': 'median of 3 solves per mode after one short warm-up solve'}
     for mode in ('fp64', 'mixed'):
         rq.ground_locg(op, x0, maxiter=3, mode=mode)   # warm-up
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        e, vec, it = rq.ground_locg(op, x0, mode=mode)
-        torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
-        res[mode] = {'time_to_e0_s': dt, 'eigval': e, 'niter': it,
-                     'residual': rq.ground_locg.last_residual}
+        runs = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            e, vec, it = rq.ground_locg(op, x0, mode=mode)
+            torch.cuda.synchronize()
+            runs.append(time.perf_counter() - t0)
+        res[mode] = {'time_to_e0_s': statistics.median(runs), 'runs_s': runs, 'eigval': e,
+                     'niter': it, 'residual': rq.ground_locg.last_residual}
     e64 = res['fp64']['eigval']
     res['mixed']['rel_err_vs_fp64'] = abs(res['mixed']['eigval'] - e64) / abs(e64)
     res['speedup_mixed_vs_fp64'] = res['fp64']['time_to_e0_s'] / res['mixed']['time_to_e0_s']

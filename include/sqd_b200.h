@@ -51,6 +51,11 @@ typedef struct sqd_op_s* sqd_op_t;
 /* ---------------------------------------------------------------- library ------------------ */
 const char* sqd_version(void);
 const char* sqd_last_error(void);
+/* The library allocates its tables and solver work vectors from its own stream-ordered memory
+ * pool per device, which keeps freed memory for reuse (no counterpart in rqutils, where XLA
+ * owns device memory).  This releases all but keep_bytes of the current device's pool back to
+ * the driver (synchronizes the device). */
+int sqd_trim_memory(uint64_t keep_bytes);
 
 /* ---------------------------------------------------------------- Pauli sums --------------- */
 /* PauliSumXZ.from_paulisum (paulis/symplectic.py:50-124), on the device: drops zero
@@ -104,10 +109,11 @@ int sqd_op_create(sqd_paulis_t p, sqd_space_t s, int x_cache, int z_cache, int l
  * matrix elements. */
 int sqd_op_info(sqd_op_t op, int64_t* nnz, int64_t* states_size, int* value_complex);
 /* Tuning knob of the cached matvec (no rqutils counterpart; rqutils leaves the schedule to
- * XLA): lanes of a warp that share one output row, 1/2/4/8/16/32.  Chosen from the mean row
- * length at creation; the autotuner overrides it. */
-int sqd_op_set_lanes(sqd_op_t op, int lanes_per_row);
-int sqd_op_get_lanes(sqd_op_t op, int* lanes_per_row);
+ * XLA): lanes of a warp that share one output row, 1/2/4/8/16/32, kept separately for FP64
+ * (precision 0: SQD_F64/SQD_C128) and FP32 (precision 1: SQD_F32/SQD_C64) vectors.  Chosen
+ * from the mean row length at creation; the autotuner overrides it. */
+int sqd_op_set_lanes(sqd_op_t op, int precision, int lanes_per_row);
+int sqd_op_get_lanes(sqd_op_t op, int precision, int* lanes_per_row);
 /* Hv on the subspace (apply_h_x_cached and friends, sqd.py:643-743 via
  * make_x_cached_matvec sqd.py:746-751).  v and out have states_size elements of dtype. */
 int sqd_matvec(sqd_op_t op, const void* v, void* out, int dtype, void* stream);

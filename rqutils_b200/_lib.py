@@ -60,9 +60,10 @@ PROTOTYPES = {
 }
 # Library extensions beyond the header's core set (declared in the header as well).
 EXTRA_PROTOTYPES = {
-    'sqd_op_set_lanes': (_i32, [_vp, _i32]),
-    'sqd_op_get_lanes': (_i32, [_vp, _c.POINTER(_i32)]),
+    'sqd_op_set_lanes': (_i32, [_vp, _i32, _i32]),
+    'sqd_op_get_lanes': (_i32, [_vp, _i32, _c.POINTER(_i32)]),
     'sqd_vinit_noalloc': (_i32, [_vp, _c.POINTER(_i64), _vp]),
+    'sqd_trim_memory': (_i32, [_u64]),
 }
 
 
@@ -100,6 +101,11 @@ def check(status):
 
 def call(name, *args):
     check(getattr(load(), name)(*args))
+
+
+def trim_memory(keep_bytes=0):
+    """Return the library's cached device memory to the driver."""
+    call('sqd_trim_memory', int(keep_bytes))
 
 
 def require_cuda():

@@ -1,9 +1,10 @@
 """Autotuner for the matvec schedule and lookup method.
 
 ``tune_lanes`` times the cached matvec for every lanes-per-row choice (the number of warp
-lanes that share one output row) with CUDA events and keeps the fastest; ``tune_lookup``
-compares the hash-table and binary-search lookups on the connectivity build.  Results are
-cached per operator shape (rows, stored pairs, cache strategy, dtype) for the process.
+lanes that share one output row) with CUDA events and keeps the fastest for the precision of
+the given vector dtype; ``tune_lookup`` compares the hash-table and binary-search lookups on the
+connectivity build.  Results are cached per operator shape (rows, stored pairs, cache strategy,
+dtype) for the process.
 """
 import torch
 
@@ -26,18 +27,21 @@ def _time(fn, reps):
 def tune_lanes(op, dtype, candidates=(2, 4, 8, 16, 32), reps=5):
     if op.cache_strategy[0] != 1:
         return {'lanes_per_row': None, 'note': 'uncached matvec has a fixed schedule'}
+    if op.value_complex and not dtype.is_complex:
+        dtype = torch.complex128 if dtype == torch.float64 else torch.complex64
+    precision = 0 if dtype in (torch.float64, torch.complex128) else 1
     key = (op.size, op.nnz, op.cache_strategy, dtype)
     if key in _CACHE:
-        op.lanes_per_row = _CACHE[key]['lanes_per_row']
+        op.set_lanes(precision, _CACHE[key]['lanes_per_row'])
         return _CACHE[key]
     v = torch.randn(op.size, dtype=dtype, device=op.space.device)
     out = torch.empty_like(v)
     times = {}
     for lpr in candidates:
-        op.lanes_per_row = lpr
+        op.set_lanes(precision, lpr)
         times[lpr] = _time(lambda: op.matvec(v, out), reps)
     best = min(times, key=times.get)
-    op.lanes_per_row = best
+    op.set_lanes(precision, best)
     res = {'lanes_per_row': best, 'ms': {str(k): round(t, 4) for k, t in times.items()}}
     _CACHE[key] = res
     return res

@@ -1,12 +1,47 @@
-// Library-level C ABI: version string and the per-thread last error message.
+// Library-level C ABI: version string, the per-thread last error message, and the library's
+// device memory pools.
+#include <cstdint>
+#include <mutex>
+
 #include "common.cuh"
 
 namespace sqd {
 namespace {
 thread_local std::string g_last_error;
-}
+constexpr int kMaxDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[kMaxDevices] = {};
+}  // namespace
+
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+cudaMemPool_t library_pool() {
+  int dev = 0;
+  SQD_CUDA(cudaGetDevice(&dev));
+  SQD_REQUIRE(dev >= 0 && dev < kMaxDevices, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    SQD_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t threshold = UINT64_MAX;
+    SQD_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    g_pools[dev] = pool;
+  }
+  return g_pools[dev];
+}
 }  // namespace sqd
+
+extern "C" int sqd_trim_memory(uint64_t keep_bytes) {
+  return sqd::guarded([&] {
+    SQD_CUDA(cudaDeviceSynchronize());
+    SQD_CUDA(cudaMemPoolTrimTo(sqd::library_pool(), static_cast<size_t>(keep_bytes)));
+  });
+}
 
 extern "C" const char* sqd_version(void) { return "sqd_b200 0.1.0 (sm_100a)"; }
 

@@ -60,8 +60,11 @@ int guarded(F&& f) {
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // ------------------------------------------------------------------------------------------
-// Stream-ordered device buffers.
+// Stream-ordered device buffers, allocated from a library-owned memory pool per device that
+// keeps freed memory for reuse (release threshold = unlimited); sqd_trim_memory returns it.
 // ------------------------------------------------------------------------------------------
+cudaMemPool_t library_pool();
+
 template <typename T>
 struct DevBuf {
   T* ptr = nullptr;
@@ -87,7 +90,8 @@ struct DevBuf {
     stream = s;
     count = n;
     if (n == 0) return;
-    cudaError_t err = cudaMallocAsync(reinterpret_cast<void**>(&ptr), n * sizeof(T), s);
+    cudaError_t err =
+        cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ptr), n * sizeof(T), library_pool(), s);
     if (err != cudaSuccess) {
       ptr = nullptr;
       count = 0;

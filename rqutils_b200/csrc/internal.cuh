@@ -58,7 +58,7 @@ struct sqd_op_s {
   int has_diag_group = 0;      // group 0 has x == 0
   int value_complex = 0;
   int64_t nnz = 0;
-  int lanes_per_row = 32;
+  int lanes_per_row[2] = {32, 32};  // [0]: FP64 vectors, [1]: FP32 vectors
   sqd::DevBuf<int64_t> row_ptr;   // [states_size + 1]
   sqd::DevBuf<uint32_t> cols;     // [nnz] source index of each stored pair
   sqd::DevBuf<uint32_t> grps;     // [nnz] group index of each stored pair

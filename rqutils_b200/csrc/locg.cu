@@ -12,6 +12,9 @@
 // CUDA graph with a conditional WHILE node whose condition the convergence step sets.
 //
 // Inner products always accumulate in FP64 (also for FP32 vectors).
+#include <cstdio>
+#include <cstdlib>
+
 #include "internal.cuh"
 #include "dispatch.cuh"
 
@@ -42,12 +45,15 @@ enum Post : int {
   P_SET_R_COEF,      // coef (1, -theta) for r = ax - theta x
   P_THETA_ONLY,      // theta = Re <x|ax> (refinement bookkeeping)
   P_RESET,           // clear done/converged/stall tracking (restart of a loop)
+  P_GRAM_IMPLICIT,   // fast variant: Gram of {x, y, p} with p unnormalised -> RR3, update coefs
+  P_UPDATE_NORMS,    // fast variant: |u|, |t| -> scaling + residual coefs
+  P_CONV_PROJ,       // fast variant: residual test + first projection coefs for the next step
   P_CHECK0           // reference residual test on (|r|^2, |Ax|^2) without counting an iteration
 };
 
 struct LocgDev {
   double red[16][2];     // reduction results of the last pass
-  double coef[2][10][2]; // coefficients of the next pass
+  double coef[6][10][2]; // coefficients of the next pass (output x source)
   double theta;
   double theta_prev;
   double kappa[3][2];
@@ -70,11 +76,11 @@ struct LocgDev {
 
 enum Gate : int { G_NONE = 0, G_DONE = 1, G_KEEP = 2 };
 
-template <int MAXS, int MAXD>
+template <int MAXS, int MAXD, int MAXO>
 struct LCArgs {
   int64_t n;
   const void* src[MAXS];
-  void* out[2];
+  void* out[MAXO];
   int nsrc, nout, ndot, post, gate, use_cond;
   signed char da[MAXD], db[MAXD];
   LocgDev* dev;
@@ -161,6 +167,30 @@ __device__ __forceinline__ void set_coef(LocgDev* d, int o, int k, double2 c) {
 __device__ __forceinline__ void set_coef_r(LocgDev* d, int o, int k, double c) {
   d->coef[o][k][0] = c;
   d->coef[o][k][1] = 0.0;
+}
+
+// Convergence test after an iteration (ground_locg.py:371-376), or the FP32 inner criterion.
+__device__ void conv_step(LocgDev* d, double ax2, int use_cond, cudaGraphConditionalHandle cond) {
+  const double r = sqrt(d->red[0][0]);
+  d->rnorm = r;
+  d->niter += 1;
+  bool conv;
+  if (d->inner_rtol > 0.0) {
+    conv = r < d->inner_rtol * fabs(d->theta);
+    if (r < 0.5 * d->best_r) {
+      d->best_r = r;
+      d->best_it = d->niter;
+    }
+    if (d->stall > 0 && d->niter - d->best_it > d->stall) conv = true;
+  } else {
+    const double reltol = (sqrt(ax2) - d->theta) * d->nscale;
+    conv = r < d->tol * reltol;
+  }
+  if (d->etol > 0.0 && d->niter >= 2 && fabs(d->theta - d->theta_prev) <= d->etol * fabs(d->theta))
+    conv = true;
+  d->converged = conv;
+  d->done = conv || d->niter >= d->maxiter;
+  if (use_cond) cudaGraphSetConditional(cond, d->done ? 0u : 1u);
 }
 
 __device__ void run_post(LocgDev* d, int post, int nsrc, int use_cond,
@@ -263,30 +293,9 @@ __device__ void run_post(LocgDev* d, int post, int nsrc, int use_cond,
       set_coef_r(d, 1, 1, 1.0 / sqrt(d->red[1][0]));
     } break;
     case P_CONV:
-    case P_CONV_SPLIT: {
-      const double r = sqrt(d->red[0][0]);
-      const double ax2 = post == P_CONV ? d->red[1][0] : d->axnorm2;
-      d->rnorm = r;
-      d->niter += 1;
-      bool conv;
-      if (d->inner_rtol > 0.0) {
-        conv = r < d->inner_rtol * fabs(d->theta);
-        if (r < 0.5 * d->best_r) {
-          d->best_r = r;
-          d->best_it = d->niter;
-        }
-        if (d->stall > 0 && d->niter - d->best_it > d->stall) conv = true;
-      } else {
-        const double reltol = (sqrt(ax2) - d->theta) * d->nscale;
-        conv = r < d->tol * reltol;
-      }
-      if (d->etol > 0.0 && d->niter >= 2 &&
-          fabs(d->theta - d->theta_prev) <= d->etol * fabs(d->theta))
-        conv = true;
-      d->converged = conv;
-      d->done = conv || d->niter >= d->maxiter;
-      if (use_cond) cudaGraphSetConditional(cond, d->done ? 0u : 1u);
-    } break;
+    case P_CONV_SPLIT:
+      conv_step(d, post == P_CONV ? d->red[1][0] : d->axnorm2, use_cond, cond);
+      break;
     case P_STORE_AX: d->axnorm2 = d->red[0][0]; break;
     case P_ORTH_IPS: {
       set_coef_r(d, 0, 0, 1.0);
@@ -315,21 +324,91 @@ __device__ void run_post(LocgDev* d, int post, int nsrc, int use_cond,
       d->converged = r < d->tol * reltol;
       d->done = d->converged;
     } break;
+    case P_GRAM_IMPLICIT: {
+      // red: 0 <x|Ax> 1 <y|Ay> 2 <p|Ap> 3 <y|Ax> 4 <p|Ax> 5 <p|Ay> 6 <p|p> 7 <y|p>
+      const double pp = d->red[6][0];
+      if (!(pp > 0.0)) {  // r already in span{x, y}: nothing left to improve
+        d->converged = 1;
+        d->done = 1;
+        if (use_cond) cudaGraphSetConditional(cond, 0u);
+        break;
+      }
+      const double s1 = 1.0 / sqrt(pp);
+      double2 m[3][3];
+      m[0][0] = red_c(d, 0);
+      m[1][1] = red_c(d, 1);
+      m[2][2] = cscale(red_c(d, 2), s1 * s1);
+      m[1][0] = red_c(d, 3);
+      m[2][0] = cscale(red_c(d, 4), s1);
+      m[2][1] = cscale(red_c(d, 5), s1);
+      m[0][1] = cconj(m[1][0]);
+      m[0][2] = cconj(m[2][0]);
+      m[1][2] = cconj(m[2][1]);
+      double ev;
+      double2 k[3];
+      eig3(m, &ev, k);
+      d->theta_prev = d->theta;
+      d->theta = ev;
+      const double2 k2 = cscale(k[2], s1);  // coefficient on the unnormalised p
+      // |s|^2 for s = k1 y + k2 p_hat, y and p_hat normalised, <y|p_hat> = red7 s1
+      const double2 yp = cscale(red_c(d, 7), s1);
+      const double ns = sqrt(fmax(cabs2(k[1]) + cabs2(k[2]) + 2.0 * cmul(cconj(k[1]), cmul(k[2], yp)).x, 1e-300));
+      const double2 f = cscale(k[0], 1.0 / ns);
+      for (int o = 0; o < 4; ++o)
+        for (int q = 0; q < 6; ++q) set_coef_r(d, o, q, 0.0);
+      // u (x), t (y) over (x, y, p); A u (ax), A t (ay) over (ax, ay, ap)
+      set_coef(d, 0, 0, k[0]);
+      set_coef(d, 0, 1, k[1]);
+      set_coef(d, 0, 2, k2);
+      set_coef_r(d, 1, 0, -ns);
+      set_coef(d, 1, 1, cmul(k[1], f));
+      set_coef(d, 1, 2, cmul(k2, f));
+      set_coef(d, 2, 3, k[0]);
+      set_coef(d, 2, 4, k[1]);
+      set_coef(d, 2, 5, k2);
+      set_coef_r(d, 3, 3, -ns);
+      set_coef(d, 3, 4, cmul(k[1], f));
+      set_coef(d, 3, 5, cmul(k2, f));
+    } break;
+    case P_UPDATE_NORMS: {
+      // red: 0 |u|^2, 1 |t|^2 ; next pass sources (x=u, y=t, ax=Au, ay=At)
+      const double cu = 1.0 / sqrt(d->red[0][0]);
+      const double ct = 1.0 / sqrt(d->red[1][0]);
+      for (int o = 0; o < 5; ++o)
+        for (int q = 0; q < 4; ++q) set_coef_r(d, o, q, 0.0);
+      set_coef_r(d, 0, 0, cu);
+      set_coef_r(d, 1, 1, ct);
+      set_coef_r(d, 2, 2, cu);
+      set_coef_r(d, 3, 3, ct);
+      set_coef_r(d, 4, 0, -d->theta * cu);
+      set_coef_r(d, 4, 2, cu);
+    } break;
+    case P_CONV_PROJ: {
+      // red: 0 |r|^2, 1 |Ax|^2, 2 <x|r>, 3 <y|r>
+      conv_step(d, d->red[1][0], use_cond, cond);
+      for (int q = 0; q < 3; ++q) {
+        d->coef[0][q][0] = 0.0;
+        d->coef[0][q][1] = 0.0;
+      }
+      set_coef_r(d, 0, 0, 1.0);
+      set_coef(d, 0, 1, make_double2(-d->red[2][0], -d->red[2][1]));
+      set_coef(d, 0, 2, make_double2(-d->red[3][0], -d->red[3][1]));
+    } break;
     default: break;
   }
 }
 
 // ----------------------------------------------------------------------------- fused pass
-template <typename R, int NC, int MAXS, int MAXD>
-__global__ void __launch_bounds__(LC_THREADS) k_lc(LCArgs<MAXS, MAXD> a) {
+template <typename R, int NC, int MAXS, int MAXD, int MAXO>
+__global__ void __launch_bounds__(LC_THREADS) k_lc(LCArgs<MAXS, MAXD, MAXO> a) {
   LocgDev* dev = a.dev;
   if ((a.gate & G_DONE) && *(volatile int*)&dev->done) return;
   if ((a.gate & G_KEEP) && *(volatile int*)&dev->keep) return;
-  double2 c[2][MAXS];
-#pragma unroll
-  for (int o = 0; o < 2; ++o)
-#pragma unroll
-    for (int k = 0; k < MAXS; ++k) c[o][k] = make_double2(dev->coef[o][k][0], dev->coef[o][k][1]);
+  __shared__ double2 sc[MAXO][MAXS];
+  for (int t = threadIdx.x; t < MAXO * MAXS; t += blockDim.x)
+    sc[t / MAXS][t % MAXS] = make_double2(dev->coef[t / MAXS][t % MAXS][0],
+                                          dev->coef[t / MAXS][t % MAXS][1]);
+  __syncthreads();
   double acc[MAXD][2];
 #pragma unroll
   for (int d = 0; d < MAXD; ++d) acc[d][0] = acc[d][1] = 0.0;
@@ -339,21 +418,20 @@ __global__ void __launch_bounds__(LC_THREADS) k_lc(LCArgs<MAXS, MAXD> a) {
     double2 s[MAXS];
 #pragma unroll
     for (int k = 0; k < MAXS; ++k) {
+      s[k] = make_double2(0.0, 0.0);
       if (k < a.nsrc) {
         const Cx<R> v = ld_elem_rw<R, NC>(static_cast<const R*>(a.src[k]), i);
         s[k] = make_double2(double(v.re), double(v.im));
-      } else {
-        s[k] = make_double2(0.0, 0.0);
       }
     }
-    double2 o[2];
+    double2 o[MAXO];
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < MAXO; ++q) {
       o[q] = make_double2(0.0, 0.0);
       if (q < a.nout) {
 #pragma unroll
         for (int k = 0; k < MAXS; ++k)
-          if (k < a.nsrc) o[q] = cadd(o[q], cmul(c[q][k], s[k]));
+          if (k < a.nsrc) o[q] = cadd(o[q], cmul(sc[q][k], s[k]));
         if constexpr (NC == 1) o[q].y = 0.0;
       }
     }
@@ -368,7 +446,7 @@ __global__ void __launch_bounds__(LC_THREADS) k_lc(LCArgs<MAXS, MAXD> a) {
           if (cb == k) y = s[k];
         }
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
+        for (int q = 0; q < MAXO; ++q) {
           if (ca == 100 + q) x = o[q];
           if (cb == 100 + q) y = o[q];
         }
@@ -378,7 +456,7 @@ __global__ void __launch_bounds__(LC_THREADS) k_lc(LCArgs<MAXS, MAXD> a) {
       }
     }
 #pragma unroll
-    for (int q = 0; q < 2; ++q)
+    for (int q = 0; q < MAXO; ++q)
       if (q < a.nout && a.out[q] != nullptr)
         st_elem<R, NC>(static_cast<R*>(a.out[q]), i, cx_make<R>(R(o[q].x), R(o[q].y)));
   }
@@ -448,8 +526,9 @@ struct Vec {
 template <typename R, int NC>
 class Locg {
  public:
-  using Small = LCArgs<6, 6>;
-  using Large = LCArgs<kMaxOrth + 1, kMaxOrth>;
+  using Tiny = LCArgs<3, 3, 2>;
+  using Wide = LCArgs<6, 10, 5>;
+  using Orth = LCArgs<kMaxOrth + 1, kMaxOrth, 2>;
 
   Locg(int64_t n, sqd_matvec_fn fn, void* ctx, cudaStream_t st)
       : n_(n), fn_(fn), ctx_(ctx), st_(st), cur_(st) {
@@ -457,7 +536,7 @@ class Locg {
       b->alloc(static_cast<size_t>(n) * NC, st);
     blocks_ = static_cast<unsigned>(
         std::max<int64_t>(1, std::min<int64_t>((n + LC_THREADS - 1) / LC_THREADS,
-                                               4 * num_sms())));
+                                               8 * num_sms())));
     partials_.alloc(static_cast<size_t>(blocks_) * 2 * 16, st);
     counter_.alloc(1, st);
     dev_.alloc(1, st);
@@ -466,6 +545,10 @@ class Locg {
     SQD_CUDA(cudaMallocHost(reinterpret_cast<void**>(&host_), sizeof(LocgDev)));
   }
   ~Locg() {
+    for (int v = 0; v < 2; ++v) {
+      if (exec_[v]) cudaGraphExecDestroy(exec_[v]);
+      if (graph_[v]) cudaGraphDestroy(graph_[v]);
+    }
     if (host_) cudaFreeHost(host_);
   }
 
@@ -490,24 +573,30 @@ class Locg {
   // ---- one fused pass
   void lc(std::initializer_list<const void*> srcs, std::initializer_list<void*> outs,
           std::initializer_list<std::pair<int, int>> dots, int post, int gate = G_NONE) {
-    if (srcs.size() <= 6 && dots.size() <= 6) {
-      Small a{};
+    if (srcs.size() <= 3 && dots.size() <= 3 && outs.size() <= 2) {
+      Tiny a{};
       fill(a, srcs, outs, dots, post, gate);
-      k_lc<R, NC, 6, 6><<<blocks_, LC_THREADS, 0, cur_>>>(a);
+      k_lc<R, NC, 3, 3, 2><<<blocks_, LC_THREADS, 0, cur_>>>(a);
+    } else if (srcs.size() <= 6 && dots.size() <= 10 && outs.size() <= 5) {
+      Wide a{};
+      fill(a, srcs, outs, dots, post, gate);
+      k_lc<R, NC, 6, 10, 5><<<blocks_, LC_THREADS, 0, cur_>>>(a);
     } else {
-      Large a{};
+      SQD_REQUIRE(srcs.size() <= kMaxOrth + 1 && dots.size() <= kMaxOrth && outs.size() <= 2,
+                  "fused pass too wide");
+      Orth a{};
       fill(a, srcs, outs, dots, post, gate);
-      k_lc<R, NC, kMaxOrth + 1, kMaxOrth><<<blocks_, LC_THREADS, 0, cur_>>>(a);
+      k_lc<R, NC, kMaxOrth + 1, kMaxOrth, 2><<<blocks_, LC_THREADS, 0, cur_>>>(a);
     }
     SQD_CHECK_LAUNCH();
   }
 
   // Runs only the scalar step `post` (one thread).
   void post_only(int post, int gate = G_NONE) {
-    Small a{};
+    Tiny a{};
     fill(a, {}, {}, {}, post, gate);
     a.n = 0;
-    k_lc<R, NC, 6, 6><<<1, LC_THREADS, 0, cur_>>>(a);
+    k_lc<R, NC, 3, 3, 2><<<1, LC_THREADS, 0, cur_>>>(a);
     SQD_CHECK_LAUNCH();
   }
 
@@ -632,24 +721,26 @@ class Locg {
     lc({ax_.ptr, x}, {r_.ptr}, {{100, 100}, {0, 0}}, P_CONV);
   }
 
-  void body_implicit() {
+  // First projection coefficients of the fast variant, from the current r, x, y.
+  void proj_ips() { lc({r_.ptr, x_.ptr, y_.ptr}, {}, {{1, 0}, {2, 0}}, P_PROJ_IPS); }
+
+  // Fast implicit iteration: 5 fused passes + 1 matvec.  p is projected out of {x, y} in two
+  // rounds (the second unnormalised: its norm enters the Rayleigh-Ritz step analytically),
+  // the Gram matrix of {x, y, p} comes from the carried A x, A y and the new A p, and
+  // x, y, A x, A y, r and the next step's first projection coefficients are produced in two
+  // passes.
+  void body_fast() {
     R *x = x_.ptr, *y = y_.ptr, *r = r_.ptr, *p = p_.ptr;
     R *ax = ax_.ptr, *ay = ay_.ptr, *ap = ap_.ptr;
     const int g = G_DONE;
-    lc({r, x, y}, {}, {{1, 0}, {2, 0}}, P_PROJ_IPS, g);
     lc({r, x, y}, {p}, {{100, 100}, {1, 100}, {2, 100}}, P_PROJ_NORM_IPS, g);
-    lc({p, x, y}, {p}, {{100, 100}, {1, 100}, {2, 100}}, P_PROJ_NORM_IPS, g);
-    lc({p, x, y}, {p}, {{1, 100}, {2, 100}}, P_PROJ_IPS, g);
-    lc({p, x, y}, {p}, {{100, 100}}, P_PROJ_MASK, g);
-    lc({p}, {p}, {}, P_NONE, g | G_KEEP);
+    lc({p, x, y}, {p}, {}, P_NONE, g);
     matvec(p, ap);
-    lc({x, y, p, ax, ay, ap}, {}, {{0, 3}, {1, 4}, {2, 5}, {1, 3}, {2, 3}, {2, 4}}, P_RR3, g);
-    lc({x, y, p}, {nullptr}, {{100, 100}}, P_SNORM, g);
-    lc({ax, ay, ap}, {ax, ay}, {}, P_NONE, g);                      // A u, A t
-    lc({x, y, p}, {x, y}, {{100, 100}, {101, 101}}, P_XY_NORM, g);  // u, t
-    lc({x, y}, {x, y}, {}, P_NONE, g);
-    lc({ax, ay}, {ax, ay}, {}, P_SET_R_COEF, g);
-    lc({ax, x}, {r}, {{100, 100}, {0, 0}}, P_CONV, g);
+    lc({x, y, p, ax, ay, ap}, {},
+       {{0, 3}, {1, 4}, {2, 5}, {1, 3}, {2, 3}, {2, 4}, {2, 2}, {1, 2}}, P_GRAM_IMPLICIT, g);
+    lc({x, y, p, ax, ay, ap}, {x, y, ax, ay}, {{100, 100}, {101, 101}}, P_UPDATE_NORMS, g);
+    lc({x, y, ax, ay}, {x, y, ax, ay, r}, {{104, 104}, {102, 102}, {100, 104}, {101, 104}},
+       P_CONV_PROJ, g);
   }
 
   // Recompute A x, A y and the residual explicitly; re-runs the convergence test.
@@ -659,6 +750,7 @@ class Locg {
     matvec(y_.ptr, ay_.ptr);
     lc({ax_.ptr, x_.ptr}, {}, {{1, 0}}, P_THETA0);
     lc({ax_.ptr, x_.ptr}, {r_.ptr}, {{100, 100}, {0, 0}}, P_CONV);
+    proj_ips();
     read_host();
   }
 
@@ -675,11 +767,11 @@ class Locg {
 
   // Runs the while-loop.  use_graph: one CUDA graph with a conditional WHILE node.
   void loop(const std::vector<const void*>& orth, int maxiter, bool use_graph,
-            bool implicit = false) {
+            bool fast = false) {
     read_host();
     if (maxiter <= 0 || host_->done) return;
     auto run_body = [&] {
-      if (implicit) body_implicit();
+      if (fast) body_fast();
       else body(orth);
     };
     if (!use_graph) {
@@ -690,31 +782,36 @@ class Locg {
       }
       return;
     }
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    SQD_CUDA(cudaGraphCreate(&graph, 0));
-    try {
-      SQD_CUDA(cudaGraphConditionalHandleCreate(&cond_, graph, 1, cudaGraphCondAssignDefault));
+    const int v = fast ? 1 : 0;
+    if (!exec_[v]) {
+      // One graph per body variant, built on first use and relaunched afterwards: a conditional
+      // WHILE node whose body is one iteration captured from a private stream (the legacy
+      // default stream cannot be captured).
+      SQD_CUDA(cudaGraphCreate(&graph_[v], 0));
+      SQD_CUDA(cudaGraphConditionalHandleCreate(&cond_[v], graph_[v], 1,
+                                                cudaGraphCondAssignDefault));
       cudaGraphNodeParams cp{};
       cp.type = cudaGraphNodeTypeConditional;
-      cp.conditional.handle = cond_;
+      cp.conditional.handle = cond_[v];
       cp.conditional.type = cudaGraphCondTypeWhile;
       cp.conditional.size = 1;
       cudaGraphNode_t node;
-      SQD_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+      SQD_CUDA(cudaGraphAddNode(&node, graph_[v], nullptr, 0, &cp));
       cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
-      use_cond_ = 1;
-      // Capture on a private stream (the legacy default stream cannot be captured), launch on
-      // the caller's stream.
       cudaStream_t cap = nullptr;
       SQD_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
       cur_ = cap;
-      cudaError_t cerr = cudaStreamBeginCaptureToGraph(cap, bodyg, nullptr, nullptr, 0,
-                                                       cudaStreamCaptureModeThreadLocal);
-      if (cerr != cudaSuccess) {
+      use_cond_ = 1;
+      cond_cur_ = cond_[v];
+      auto restore = [&] {
         cur_ = st_;
         use_cond_ = 0;
         cudaStreamDestroy(cap);
+      };
+      cudaError_t cerr = cudaStreamBeginCaptureToGraph(cap, bodyg, nullptr, nullptr, 0,
+                                                       cudaStreamCaptureModeThreadLocal);
+      if (cerr != cudaSuccess) {
+        restore();
         SQD_CUDA(cerr);
       }
       try {
@@ -722,26 +819,16 @@ class Locg {
       } catch (...) {
         cudaGraph_t dummy;
         cudaStreamEndCapture(cap, &dummy);
-        cur_ = st_;
-        use_cond_ = 0;
-        cudaStreamDestroy(cap);
+        restore();
         throw;
       }
       cerr = cudaStreamEndCapture(cap, &bodyg);
-      cur_ = st_;
-      use_cond_ = 0;
-      cudaStreamDestroy(cap);
+      restore();
       SQD_CUDA(cerr);
-      SQD_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-      SQD_CUDA(cudaGraphLaunch(exec, st_));
-      read_host();
-    } catch (...) {
-      if (exec) cudaGraphExecDestroy(exec);
-      cudaGraphDestroy(graph);
-      throw;
+      SQD_CUDA(cudaGraphInstantiate(&exec_[v], graph_[v], 0));
     }
-    cudaGraphExecDestroy(exec);
-    cudaGraphDestroy(graph);
+    SQD_CUDA(cudaGraphLaunch(exec_[v], st_));
+    read_host();
   }
 
   DevBuf<R> x_, y_, r_, p_, ax_, ay_, ap_, t0_;
@@ -770,12 +857,12 @@ class Locg {
     a.partials = partials_.ptr;
     a.counter = counter_.ptr;
     a.use_cond = use_cond_;
-    a.cond = cond_;
+    a.cond = cond_cur_;
   }
   // Variant for the orth projection: sources (v, o_0, ..., o_{m-1}).
   void lc_vec(const std::vector<const void*>& orth, void* v, std::vector<void*> outs,
               const std::vector<std::pair<int, int>>& dots, int post, int gate) {
-    Large a{};
+    Orth a{};
     a.n = n_;
     a.src[0] = v;
     for (size_t k = 0; k < orth.size(); ++k) a.src[k + 1] = orth[k];
@@ -793,8 +880,8 @@ class Locg {
     a.partials = partials_.ptr;
     a.counter = counter_.ptr;
     a.use_cond = use_cond_;
-    a.cond = cond_;
-    k_lc<R, NC, kMaxOrth + 1, kMaxOrth><<<blocks_, LC_THREADS, 0, cur_>>>(a);
+    a.cond = cond_cur_;
+    k_lc<R, NC, kMaxOrth + 1, kMaxOrth, 2><<<blocks_, LC_THREADS, 0, cur_>>>(a);
     SQD_CHECK_LAUNCH();
   }
   static std::string last_msg() {
@@ -813,7 +900,10 @@ class Locg {
   DevBuf<LocgDev> dev_;
   LocgDev* host_ = nullptr;
   int use_cond_ = 0;
-  cudaGraphConditionalHandle cond_ = 0;
+  cudaGraphConditionalHandle cond_cur_ = 0;
+  cudaGraphConditionalHandle cond_[2] = {0, 0};
+  cudaGraph_t graph_[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec_[2] = {nullptr, nullptr};
 };
 
 // Matvec adapter for the FP32 phase of the mixed solver.
@@ -876,6 +966,15 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xin
   op_ensure_values32(op, st);
   OpCtx32 c32{op, NC == 2 ? SQD_C64 : SQD_F32};
   OpCtx64 c64{op, NC == 2 ? SQD_C128 : SQD_F64};
+  // Phase timing on stderr when SQD_LOCG_TRACE is set (like the reference's debug prints).
+  const bool trace = std::getenv("SQD_LOCG_TRACE") != nullptr;
+  cudaEvent_t ev[4] = {};
+  if (trace)
+    for (auto& e : ev) SQD_CUDA(cudaEventCreate(&e));
+  auto mark = [&](int k) {
+    if (trace) SQD_CUDA(cudaEventRecord(ev[k], st));
+  };
+  mark(0);
   constexpr double kInnerRtol = 2e-7;
   constexpr int kStall = 25;
   constexpr int kRestarts = 6;
@@ -893,6 +992,7 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xin
     }
     SQD_CHECK_LAUNCH();
     L.start_implicit();
+    L.proj_ips();
     for (int k = 0; k < kRestarts; ++k) {
       L.loop(orth, maxiter, use_graph, true);
       if (L.host().niter >= maxiter || L.host().rzero) break;
@@ -902,19 +1002,30 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xin
     it32 = L.host().niter;
     k_convert<double, float, NC><<<G, 256, 0, st>>>(L.x(), x64.ptr, n);
     SQD_CHECK_LAUNCH();
+    mark(1);
   }
+  // FP64 polish: fast implicit iterations (one FP64 matvec each) with the reference's
+  // residual test; in FP64 the carried products drift by O(eps) only.
   Locg<double, NC> L(n, op_cb64, &c64, st);
   const int left = std::max(1, maxiter - it32);
   L.set_params(tol < 0 ? eps64 : tol, nscale, left, 0.0, 0.0, 0);
   SQD_CUDA(cudaMemcpyAsync(L.x(), x64.ptr, sizeof(double) * NC * n, cudaMemcpyDeviceToDevice,
                            st));
-  L.check0();
-  int it64 = 0;
-  if (!L.host().converged) {
-    L.set_params(tol < 0 ? eps64 : tol, nscale, left, 0.0, 0.0, 0);
-    L.start(orth);
-    L.loop(orth, left, use_graph);
-    it64 = L.host().niter;
+  L.start_implicit();
+  L.proj_ips();
+  mark(2);
+  L.loop(orth, left, use_graph, true);
+  const int it64 = L.host().niter;
+  mark(3);
+  if (trace) {
+    SQD_CUDA(cudaEventSynchronize(ev[3]));
+    float t[3];
+    for (int k = 0; k < 3; ++k) SQD_CUDA(cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]));
+    std::fprintf(stderr,
+                 "[sqd_locg mixed] fp32 sweeps %d it %.3f ms | fp64 start %.3f ms | "
+                 "fp64 iterations %d it %.3f ms\n",
+                 it32, t[0], t[1], it64, t[2]);
+    for (auto& e : ev) cudaEventDestroy(e);
   }
   const LocgDev& h = L.host();
   *eigval = h.theta;

@@ -223,7 +223,7 @@ void op_matvec(sqd_op_s* op, const void* v, void* out, int dtype, cudaStream_t s
     const R* vin = static_cast<const R*>(v);
     R* vout = static_cast<R*>(out);
     if (op->x_cache == 1) {
-      dispatch_lpr(op->lanes_per_row, [&](auto lpr_t) {
+      dispatch_lpr(op->lanes_per_row[sizeof(R) == 8 ? 0 : 1], [&](auto lpr_t) {
         constexpr int LPR = decltype(lpr_t)::value;
         const unsigned G = mv_grid(size, LPR);
         if (op->z_cache == 2) {

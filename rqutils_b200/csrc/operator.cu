@@ -14,29 +14,37 @@
 namespace sqd {
 namespace {
 
+// Groups that can connect, split in two classes so that the class-0 groups come first in every
+// row's stored pairs.  Class 0 (two sectors only): groups acting on the high sector alone.  In
+// an alpha x beta product subspace all rows with the same beta string have the same class-0
+// connections, so a warp serving consecutive rows gathers adjacent amplitudes for them.
 __global__ void k_gpre_flags(const uint64_t* group_x, int64_t J, int nsec, uint64_t m0,
-                             uint64_t m1, int64_t* flags) {
+                             uint64_t m1, int64_t* flags0, int64_t* flags1) {
   for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < J;
        j += int64_t(gridDim.x) * blockDim.x) {
     const uint64_t x = group_x[j];
     bool ok = x != 0;
     if (nsec > 0) ok = ok && ((__popcll(x & m0) & 1) == 0);
     if (nsec > 1) ok = ok && ((__popcll(x & m1) & 1) == 0);
-    flags[j] = ok ? 1 : 0;
+    const bool first = nsec > 1 && (x & m0) == 0;
+    flags0[j] = (ok && first) ? 1 : 0;
+    flags1[j] = (ok && !first) ? 1 : 0;
   }
 }
 
-__global__ void k_gpre_fill(const uint64_t* group_x, int64_t J, const int64_t* flags,
-                            const int64_t* pos, uint64_t m0, uint64_t m1, GroupPre* out) {
+__global__ void k_gpre_fill(const uint64_t* group_x, int64_t J, const int64_t* flags0,
+                            const int64_t* pos0, const int64_t* flags1, const int64_t* pos1,
+                            uint64_t m0, uint64_t m1, GroupPre* out) {
+  const int64_t n0 = pos0[J];
   for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < J;
        j += int64_t(gridDim.x) * blockDim.x) {
-    if (!flags[j]) continue;
+    if (!flags0[j] && !flags1[j]) continue;
     const uint64_t x = group_x[j];
     GroupPre g;
     g.x = x;
     g.group = static_cast<int32_t>(j);
     g.cx = (__popcll(x & m0) & 0xff) | ((__popcll(x & m1) & 0xff) << 8);
-    out[pos[j]] = g;
+    out[flags0[j] ? pos0[j] : n0 + pos1[j]] = g;
   }
 }
 
@@ -324,18 +332,24 @@ void op_build(sqd_op_s* op, cudaStream_t st) {
 
   // Groups that can connect.
   {
-    DevBuf<int64_t> flags, pos;
-    flags.alloc(J, st);
-    pos.alloc(J + 1, st);
+    DevBuf<int64_t> flags0, pos0, flags1, pos1;
+    flags0.alloc(J, st);
+    pos0.alloc(J + 1, st);
+    flags1.alloc(J, st);
+    pos1.alloc(J + 1, st);
     const unsigned G = grid_for(J, 256, 4096);
     k_gpre_flags<<<G, 256, 0, st>>>(p->group_x.ptr, J, sp->num_sectors, sp->sector_mask[0],
-                                   sp->sector_mask[1], flags.ptr);
+                                   sp->sector_mask[1], flags0.ptr, flags1.ptr);
     SQD_CHECK_LAUNCH();
-    exclusive_scan_i64(flags.ptr, pos.ptr, J, true, st);
-    copy_to_host(&op->n_gpre, pos.ptr + J, 1, st);
+    exclusive_scan_i64(flags0.ptr, pos0.ptr, J, true, st);
+    exclusive_scan_i64(flags1.ptr, pos1.ptr, J, true, st);
+    int64_t n0 = 0, n1 = 0;
+    copy_to_host(&n0, pos0.ptr + J, 1, st);
+    copy_to_host(&n1, pos1.ptr + J, 1, st);
+    op->n_gpre = n0 + n1;
     op->gpre.alloc(op->n_gpre > 0 ? op->n_gpre : 1, st);
-    k_gpre_fill<<<G, 256, 0, st>>>(p->group_x.ptr, J, flags.ptr, pos.ptr, sp->sector_mask[0],
-                                  sp->sector_mask[1], op->gpre.ptr);
+    k_gpre_fill<<<G, 256, 0, st>>>(p->group_x.ptr, J, flags0.ptr, pos0.ptr, flags1.ptr, pos1.ptr,
+                                  sp->sector_mask[0], sp->sector_mask[1], op->gpre.ptr);
     SQD_CHECK_LAUNCH();
   }
   if (op->x_cache == 0) return;
@@ -416,7 +430,8 @@ void op_build(sqd_op_s* op, cudaStream_t st) {
   }
   // Lanes per row from the mean row length.
   const double avg = nu > 0 ? static_cast<double>(op->nnz) / static_cast<double>(nu) : 0.0;
-  op->lanes_per_row = avg >= 96 ? 32 : avg >= 40 ? 16 : avg >= 16 ? 8 : avg >= 6 ? 4 : 2;
+  const int lpr = avg >= 96 ? 32 : avg >= 40 ? 16 : avg >= 16 ? 8 : avg >= 6 ? 4 : 2;
+  op->lanes_per_row[0] = op->lanes_per_row[1] = lpr;
   SQD_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -463,18 +478,20 @@ extern "C" int sqd_op_info(sqd_op_t op, int64_t* nnz, int64_t* states_size, int*
   });
 }
 
-extern "C" int sqd_op_set_lanes(sqd_op_t op, int lanes_per_row) {
+extern "C" int sqd_op_set_lanes(sqd_op_t op, int precision, int lanes_per_row) {
   return guarded([&] {
     SQD_REQUIRE(op != nullptr, "NULL operator");
+    SQD_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (FP32)");
     dispatch_lpr(lanes_per_row, [](auto) {});
-    op->lanes_per_row = lanes_per_row;
+    op->lanes_per_row[precision] = lanes_per_row;
   });
 }
 
-extern "C" int sqd_op_get_lanes(sqd_op_t op, int* lanes_per_row) {
+extern "C" int sqd_op_get_lanes(sqd_op_t op, int precision, int* lanes_per_row) {
   return guarded([&] {
     SQD_REQUIRE(op != nullptr && lanes_per_row != nullptr, "NULL argument");
-    *lanes_per_row = op->lanes_per_row;
+    SQD_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (FP32)");
+    *lanes_per_row = op->lanes_per_row[precision];
   });
 }
 

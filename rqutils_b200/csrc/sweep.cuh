@@ -8,7 +8,8 @@
 //   3. exact lookup (hash table or binary search) of s ^ x.
 // Candidates surviving 1-2 are pushed into a per-warp FIFO in shared memory and looked up 32 at
 // a time, so the expensive step runs on full warps.  Candidates of one row enter the FIFO in
-// increasing group order, which keeps every row's entries in the reference's scan order.
+// the order of the group list, so COUNT and FILL agree and every row's pairs follow that order
+// (the high-sector-only groups first, see k_gpre_flags).
 //
 // Modes: COUNT (pairs per row), FILL (write (col, group) at the row's CSR slots), APPLY
 // (accumulate diag_j(s) * v[src] per row: the uncached matvec, cache_strategy (0, *)).

@@ -168,13 +168,22 @@ class SQDOperator:
 
     @property
     def lanes_per_row(self):
-        v = _lib._i32()
-        _lib.call('sqd_op_get_lanes', self._handle, _lib._c.byref(v))
-        return v.value
+        """Lanes per row of the FP64-vector matvec (the FP32 one: ``get_lanes(1)``)."""
+        return self.get_lanes(0)
 
     @lanes_per_row.setter
     def lanes_per_row(self, v):
-        _lib.call('sqd_op_set_lanes', self._handle, int(v))
+        self.set_lanes(0, v)
+        self.set_lanes(1, v)
+
+    def get_lanes(self, precision):
+        v = _lib._i32()
+        _lib.call('sqd_op_get_lanes', self._handle, int(precision), _lib._c.byref(v))
+        return v.value
+
+    def set_lanes(self, precision, lanes):
+        """precision 0: FP64 vectors (float64/complex128), 1: FP32 vectors."""
+        _lib.call('sqd_op_set_lanes', self._handle, int(precision), int(lanes))
 
     def matvec(self, v, out=None):
         v = v.contiguous()
@@ -223,9 +232,16 @@ class SQDOperator:
         return out
 
     def autotune(self, dtype=None, candidates=(2, 4, 8, 16, 32), reps=5):
-        """Times the matvec for each lanes-per-row choice and keeps the fastest."""
+        """Times the matvec for each lanes-per-row choice and keeps the fastest (for the
+        precision of ``dtype``; both precisions when ``dtype`` is None)."""
         from .autotune import tune_lanes
-        return tune_lanes(self, dtype or self.dtype, candidates, reps)
+        if dtype is not None:
+            return tune_lanes(self, dtype, candidates, reps)
+        cplx = True
+        return {'fp64': tune_lanes(self, torch.complex128 if cplx else torch.float64,
+                                   candidates, reps),
+                'fp32': tune_lanes(self, torch.complex64 if cplx else torch.float32,
+                                   candidates, reps)}
 
 
 def _as_pauli(hamiltonian):
