@@ -330,6 +330,8 @@ def run_ours(args):
     extra = {}
     if not args.no_locg and rank == 0:
         extra['locg'] = locg_times(rq, op, wl, dev)
+    if args.workload == 'c5' and rank == 0:
+        extra['gradient'] = gradient_check(rq, op, wl)
     line = None
     if rank == 0:
         line = {
@@ -362,6 +364,40 @@ def run_ours(args):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def gradient_check(rq, op, wl, n_coords=32, h=1e-5):
+    """dE0/dc for every raw coefficient through the autograd backward (Hellmann-Feynman),
+    against FP64 central finite differences on ``n_coords`` random coordinates."""
+    import torch
+    from rqutils_b200.autograd import ground_energy
+    coeffs = torch.as_tensor(wl.coeffs, device='cuda').clone().requires_grad_(True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e = ground_energy(coeffs, op)
+    e.backward()
+    torch.cuda.synchronize()
+    t_grad = time.perf_counter() - t0
+    grad = coeffs.grad.detach().cpu().numpy()
+    rng = np.random.default_rng(5)
+    ks = rng.choice(len(wl.coeffs), size=n_coords, replace=False)
+    errs = []
+    t0 = time.perf_counter()
+    for k in ks:
+        cp = wl.coeffs.copy()
+        cm = wl.coeffs.copy()
+        cp[k] += h
+        cm[k] -= h
+        ep = ground_energy(torch.as_tensor(cp, device='cuda'), op).item()
+        em = ground_energy(torch.as_tensor(cm, device='cuda'), op).item()
+        fd = (ep - em) / (2 * h)
+        errs.append(abs(fd - grad[k]) / max(abs(fd), 1e-12))
+    t_fd = time.perf_counter() - t0
+    ground_energy(torch.as_tensor(wl.coeffs, device='cuda'), op)   # restore
+    return {'energy': e.item(), 'num_coeffs': int(len(wl.coeffs)),
+            'time_energy_and_gradient_s': t_grad, 'fd_coords': int(n_coords), 'fd_step': h,
+            'fd_time_s': t_fd, 'max_rel_err_vs_fd': float(max(errs)),
+            'median_rel_err_vs_fd': float(np.median(errs))}
 
 
 def locg_times(rq, op, wl, dev):

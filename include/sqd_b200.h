@@ -75,6 +75,14 @@ int sqd_paulis_info(sqd_paulis_t p, int64_t* num_groups, int64_t* num_terms, int
  * raw_to_term[num_raw] (int32, -1 for dropped zero coefficients). */
 int sqd_paulis_export(sqd_paulis_t p, uint64_t* group_x, int64_t* group_start, uint64_t* term_z,
                       double* term_c, int32_t* raw_to_term, void* stream);
+/* New coefficients for the same num_raw_terms terms (same order as at creation), keeping the
+ * grouping: merged sums, phases and the per-group stop at the first zero coefficient are
+ * recomputed as in sqd_paulis_create.  Terms dropped at creation (zero coefficient) must stay
+ * zero, and a real sum must stay real; otherwise SQD_ERR_INVALID.  Operators built on p need
+ * sqd_op_refresh afterwards.  No rqutils counterpart (rqutils rebuilds the PauliSumXZ); used by
+ * the coefficient-gradient path. */
+int sqd_paulis_set_coeffs(sqd_paulis_t p, const double* coef_re, const double* coef_im,
+                          void* stream, int* imag_dropped_host);
 void sqd_paulis_destroy(sqd_paulis_t p);
 
 /* ---------------------------------------------------------------- subspace ----------------- */
@@ -139,6 +147,9 @@ int sqd_op_csr(sqd_op_t op, int64_t* indptr, int32_t* indices, double* data, voi
  * t-th Pauli string with unit coefficient, projected), FP64; u, v of dtype (SQD_F64/C128). */
 int sqd_grad_terms(sqd_op_t op, const void* u, const void* v, int dtype, double* out_terms,
                    void* stream);
+/* Recomputes the cached matrix elements (cache z = 2) after sqd_paulis_set_coeffs; the
+ * connectivity is unchanged. */
+int sqd_op_refresh(sqd_op_t op, void* stream);
 void sqd_op_destroy(sqd_op_t op);
 
 /* ---------------------------------------------------------------- LOCG --------------------- */

@@ -64,6 +64,8 @@ EXTRA_PROTOTYPES = {
     'sqd_op_get_lanes': (_i32, [_vp, _i32, _c.POINTER(_i32)]),
     'sqd_vinit_noalloc': (_i32, [_vp, _c.POINTER(_i64), _vp]),
     'sqd_trim_memory': (_i32, [_u64]),
+    'sqd_paulis_set_coeffs': (_i32, [_vp, _vp, _vp, _vp, _c.POINTER(_i32)]),
+    'sqd_op_refresh': (_i32, [_vp, _vp]),
 }
 
 

@@ -20,6 +20,12 @@ struct sqd_paulis_s {
   sqd::DevBuf<double> term_c;         // [2M] interleaved (re, im)
   sqd::DevBuf<int32_t> term_group;    // [M]
   sqd::DevBuf<int32_t> raw_to_term;   // [num_raw]
+  // term -> raw terms merged into it, in input order (for coefficient updates)
+  int64_t num_kept = 0;
+  uint32_t flags = 0;
+  sqd::DevBuf<int64_t> term_raw_start;  // [M + 1] into term_raw
+  sqd::DevBuf<uint32_t> term_raw;       // [num_kept] raw indices
+  sqd::DevBuf<uint64_t> term_x;         // [M]
 };
 
 // Sorted unique subspace plus lookup structures.

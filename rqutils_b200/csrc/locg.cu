@@ -207,6 +207,13 @@ __device__ void run_post(LocgDev* d, int post, int nsrc, int use_cond,
       d->rnorm = sqrt(d->red[0][0]);
       d->rzero = d->rnorm == 0.0;
       set_coef_r(d, 0, 0, 1.0 / d->rnorm);
+      // The start vector is an exact eigenvector.  The reference carries on into its loop body
+      // and divides 0/0 (|s| = 0, ground_locg.py:336-338), returning NaN; here the exact
+      // eigenpair is returned instead.
+      if (d->rzero) {
+        d->converged = 1;
+        d->done = 1;
+      }
     } break;
     case P_RR2: {
       double2 m[2][2];

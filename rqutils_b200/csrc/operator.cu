@@ -579,6 +579,36 @@ extern "C" int sqd_op_csr(sqd_op_t op, int64_t* indptr, int32_t* indices, double
   });
 }
 
+extern "C" int sqd_op_refresh(sqd_op_t op, void* stream) {
+  return guarded([&] {
+    SQD_REQUIRE(op != nullptr, "NULL operator");
+    sqd_paulis_s* p = op->p;
+    sqd_space_s* sp = op->s;
+    SQD_REQUIRE(p->is_complex == op->value_complex,
+                "the Pauli sum changed between real and complex; create a new operator");
+    if (op->z_cache != 2 || op->nnz == 0) return;
+    cudaStream_t st = as_stream(stream);
+    const int64_t size = sp->states_size;
+    const unsigned G = grid_for(size * 32, 256, 16384);
+    if (op->value_complex)
+      k_values<2><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->grps.ptr, sp->states.ptr,
+                                     sp->n_unique, sp->fill_state, size, p->group_start.ptr,
+                                     p->group_eff.ptr, p->term_z.ptr, p->term_c.ptr,
+                                     op->values.ptr, 0);
+    else
+      k_values<1><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->grps.ptr, sp->states.ptr,
+                                     sp->n_unique, sp->fill_state, size, p->group_start.ptr,
+                                     p->group_eff.ptr, p->term_z.ptr, p->term_c.ptr,
+                                     op->values.ptr, 0);
+    SQD_CHECK_LAUNCH();
+    if (op->values32.ptr) {
+      const size_t n = static_cast<size_t>(op->nnz) * (op->value_complex ? 2 : 1);
+      k_to_float<<<grid_for(n, 256, 16384), 256, 0, st>>>(op->values.ptr, op->values32.ptr, n);
+      SQD_CHECK_LAUNCH();
+    }
+  });
+}
+
 extern "C" int sqd_grad_terms(sqd_op_t op, const void* u, const void* v, int dtype,
                               double* out_terms, void* stream) {
   return guarded([&] {

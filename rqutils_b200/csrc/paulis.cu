@@ -183,12 +183,16 @@ extern "C" int sqd_paulis_create(const uint64_t* x, const uint64_t* z, const dou
     copy_to_host(&m, term_pos.ptr + n_kept, 1, st);
     p->num_terms = m;
 
-    DevBuf<int64_t> term_item_start;
-    term_item_start.alloc(m, st);
+    DevBuf<int64_t>& term_item_start = p->term_raw_start;
+    term_item_start.alloc(m + 1, st);
     k_term_starts<<<Gk, B, 0, st>>>(new_term.ptr, term_pos.ptr, n_kept, term_item_start.ptr);
     SQD_CHECK_LAUNCH();
+    SQD_CUDA(cudaMemcpyAsync(term_item_start.ptr + m, &n_kept, sizeof(int64_t),
+                             cudaMemcpyHostToDevice, st));
+    p->num_kept = n_kept;
+    p->flags = flags;
 
-    DevBuf<uint64_t> term_x;
+    DevBuf<uint64_t>& term_x = p->term_x;
     DevBuf<int> flags_dev;
     term_x.alloc(m, st);
     p->term_z.alloc(m, st);
@@ -237,7 +241,91 @@ extern "C" int sqd_paulis_create(const uint64_t* x, const uint64_t* z, const dou
     p->is_complex = hflags[1];
     p->max_k = static_cast<int64_t>(hmax);
     if (imag_dropped_host) *imag_dropped_host = hflags[0];
+    p->term_raw.swap(idx);
     *out = p.release();
+  });
+}
+
+namespace sqd {
+namespace {
+
+// New coefficients for the same terms: merged sums in input order, phase, as at creation.
+__global__ void k_set_coeffs(const int64_t* trs, const uint32_t* tr, int64_t m,
+                             const uint64_t* term_x, const uint64_t* term_z, const double* re,
+                             const double* im, int force_real, double* term_c, int* flags) {
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < m;
+       t += int64_t(gridDim.x) * blockDim.x) {
+    double sr = 0.0, si = 0.0;
+    for (int64_t i = trs[t]; i < trs[t + 1]; ++i) {
+      sr += re[tr[i]];
+      if (im) si += im[tr[i]];
+    }
+    if (force_real) {
+      if (si != 0.0) atomicExch(flags, 1);
+      si = 0.0;
+    }
+    const int ph = __popcll(term_x[t] & term_z[t]) & 3;
+    double cr, ci;
+    switch (ph) {
+      case 0: cr = sr; ci = si; break;
+      case 1: cr = si; ci = -sr; break;
+      case 2: cr = -sr; ci = -si; break;
+      default: cr = -si; ci = sr; break;
+    }
+    term_c[2 * t] = cr;
+    term_c[2 * t + 1] = ci;
+    if (ci != 0.0) atomicExch(flags + 1, 1);
+  }
+}
+
+// A raw term dropped at creation (zero coefficient) must stay zero: the table has no slot.
+__global__ void k_check_dropped(const int32_t* raw_to_term, const double* re, const double* im,
+                                int64_t n, int* flag) {
+  for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n;
+       r += int64_t(gridDim.x) * blockDim.x)
+    if (raw_to_term[r] < 0 && (re[r] != 0.0 || (im != nullptr && im[r] != 0.0)))
+      atomicExch(flag, 1);
+}
+
+}  // namespace
+}  // namespace sqd
+
+extern "C" int sqd_paulis_set_coeffs(sqd_paulis_t p, const double* coef_re,
+                                     const double* coef_im, void* stream,
+                                     int* imag_dropped_host) {
+  return guarded([&] {
+    SQD_REQUIRE(p != nullptr && coef_re != nullptr, "NULL argument");
+    cudaStream_t st = as_stream(stream);
+    const int B = 256;
+    DevBuf<int> flags;
+    flags.alloc(3, st);
+    SQD_CUDA(cudaMemsetAsync(flags.ptr, 0, 3 * sizeof(int), st));
+    k_check_dropped<<<grid_for(p->num_raw, B, 4096), B, 0, st>>>(
+        p->raw_to_term.ptr, coef_re, coef_im, p->num_raw, flags.ptr + 2);
+    SQD_CHECK_LAUNCH();
+    int h[3];
+    copy_to_host(h, flags.ptr, 3, st);
+    SQD_REQUIRE(h[2] == 0,
+                "a term whose coefficient was zero when the Pauli sum was created became nonzero; "
+                "create a new Pauli sum");
+    DevBuf<double> newc;
+    newc.alloc(2 * p->num_terms, st);
+    k_set_coeffs<<<grid_for(p->num_terms, B, 4096), B, 0, st>>>(
+        p->term_raw_start.ptr, p->term_raw.ptr, p->num_terms, p->term_x.ptr, p->term_z.ptr,
+        coef_re, coef_im, (p->flags & SQD_PAULIS_FORCE_REAL) ? 1 : 0, newc.ptr, flags.ptr);
+    SQD_CHECK_LAUNCH();
+    copy_to_host(h, flags.ptr, 2, st);
+    SQD_REQUIRE(h[1] == 0 || p->is_complex,
+                "new coefficients make a real Hamiltonian complex; create a new Pauli sum");
+    SQD_CUDA(cudaMemcpyAsync(p->term_c.ptr, newc.ptr, newc.bytes(), cudaMemcpyDeviceToDevice, st));
+    DevBuf<unsigned long long> maxk;
+    maxk.alloc(1, st);
+    SQD_CUDA(cudaMemsetAsync(maxk.ptr, 0, sizeof(unsigned long long), st));
+    k_group_eff<<<grid_for(p->num_groups, B, 4096), B, 0, st>>>(
+        p->group_start.ptr, p->term_c.ptr, p->num_groups, p->group_eff.ptr, maxk.ptr);
+    SQD_CHECK_LAUNCH();
+    SQD_CUDA(cudaStreamSynchronize(st));
+    if (imag_dropped_host) *imag_dropped_host = h[0];
   });
 }
 

@@ -123,6 +123,29 @@ class PauliSumXZ:
         obj._num_raw = x.shape[0]
         return obj
 
+    def set_coeffs(self, coeffs):
+        """New coefficients for the raw terms this sum was created from (same order); the
+        grouping is kept.  Operators built on this sum need ``SQDOperator.refresh()``."""
+        coeffs = torch.as_tensor(coeffs)
+        if coeffs.shape[0] != self._num_raw:
+            raise ValueError('Lengths of Pauli and coeff lists do not match')
+        re = coeffs.real if coeffs.is_complex() else coeffs
+        re = re.to(device=self._device, dtype=torch.float64).contiguous()
+        im = None
+        if coeffs.is_complex():
+            im = coeffs.imag.to(device=self._device, dtype=torch.float64).contiguous()
+        dropped = _lib._c.c_int(0)
+        _lib.call('sqd_paulis_set_coeffs', self._handle, _lib.ptr(re), _lib.ptr(im),
+                  _lib.stream_ptr(), _lib._c.byref(dropped))
+        if dropped.value:
+            warnings.warn('Found nonzero imaginary part when force_real=True')
+        self._cache.pop('tables', None)
+        self._cache.pop('ref', None)
+
+    def raw_to_term(self):
+        """int64 CUDA tensor: merged-term index of every raw term (-1 if dropped)."""
+        return self.device_tables()[4].to(torch.int64)
+
     def __del__(self):
         h = getattr(self, '_handle', None)
         if h is not None and h.value:

@@ -219,6 +219,10 @@ class SQDOperator:
                   _lib.ptr(data), _lib.stream_ptr())
         return indptr, indices, data
 
+    def refresh(self):
+        """Recompute the cached matrix elements after ``hamiltonian.set_coeffs``."""
+        _lib.call('sqd_op_refresh', self._handle, _lib.stream_ptr())
+
     def grad_terms(self, u, v):
         """Re <u|P_t|v> for every merged term t (FP64 CUDA tensor of num_terms)."""
         out = torch.empty(self.hamiltonian.num_terms, dtype=torch.float64,

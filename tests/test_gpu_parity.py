@@ -277,3 +277,53 @@ def test_gradient_terms_match_hellmann_feynman_oracle():
     np.testing.assert_allclose(g.cpu().numpy(), ref, rtol=1e-10, atol=1e-9)
     # autograd-style check of one coordinate: d<v|H|v>/d alpha_t = g_t
     assert np.isfinite(ref).all()
+
+
+def test_exact_eigenvector_start_returns_exact_pair():
+    # Diagonal Hamiltonian: the one-hot vinit is an exact eigenvector (r = 0 after iteration 0).
+    labels = ['ZIII', 'IZZI', 'IIZZ', 'ZIIZ']
+    coeffs = [0.7, -1.1, 0.4, -0.3]
+    states = OQ.u64_to_states(np.arange(16, dtype=np.uint64), 4)
+    e, vec, basis = rq.sqd((labels, coeffs), states)
+    dense = OD.projected_matrix(labels, coeffs, np.arange(16))
+    assert np.isfinite(e) and abs(e - np.linalg.eigvalsh(dense)[0]) < 1e-14
+    assert np.isfinite(vec).all()
+
+
+def test_duplicate_and_unsorted_inputs_with_fill_slots():
+    rng = np.random.default_rng(12)
+    x, z, c = W.random_pauli_sum(9, 50, rng)
+    labels = W.labels_from_xz(x, z, 9)
+    base = W.weight_subspace(9, 4, 90, rng)
+    sample = np.concatenate([base, base[:30], base[::-1]])
+    bits = OQ.u64_to_states(sample, 9)
+    size = bits.shape[0] + 5
+    e, vec, basis = rq.sqd((labels, list(c)), bits, states_size=size,
+                           options={'locg_tol': 1e-13})
+    eo, veco, basiso = OQ.sqd((labels, list(c)), bits, states_size=size,
+                              options={'locg_tol': 1e-13})
+    assert (basis == basiso).all() and basis.shape[0] == 90
+    assert abs(e - eo) <= 1e-10 * abs(eo)
+    assert abs(abs(np.vdot(vec, veco)) - 1) < 1e-8
+
+
+def test_sqd_reference_layout_pauli_input():
+    g = golden('sqd_small')
+    ref = OS.from_paulisum((labels_of(g), list(g['coeffs'])), force_real=True, add_padding=True)
+    ham = rq.PauliSumXZ(ref.x, ref.z, ref.c, 10)
+    e = rq.sqd(ham, g['states'], states_size=int(g['states_size']),
+               options={'locg_tol': 1e-12, 'return_eigvec': False})
+    assert abs(e - float(g['eig_dense'])) <= ENERGY_RTOL * abs(float(g['eig_dense']))
+
+
+def test_invalid_inputs_raise_value_error():
+    with pytest.raises(ValueError):
+        rq.PauliSumXZ.from_xz(np.array([1], dtype=np.uint64), np.array([0], dtype=np.uint64),
+                              np.array([0.0]), 4)       # every coefficient is zero
+    with pytest.raises(ValueError):
+        rq.Subspace.from_u64(np.array([1 << 9], dtype=np.uint64), 8)   # bit above num_qubits
+    ham = rq.PauliSumXZ.from_xz(np.array([1], dtype=np.uint64), np.array([0], dtype=np.uint64),
+                                np.array([1.0]), 8)
+    space = rq.Subspace.from_u64(np.arange(4, dtype=np.uint64), 9)
+    with pytest.raises(ValueError, match='qubits'):
+        rq.SQDOperator(ham, space)
