@@ -47,6 +47,7 @@ enum sqd_lookup { SQD_LOOKUP_HASH = 0, SQD_LOOKUP_BSEARCH = 1 };
 typedef struct sqd_paulis_s* sqd_paulis_t;
 typedef struct sqd_space_s* sqd_space_t;
 typedef struct sqd_op_s* sqd_op_t;
+typedef struct sqd_batch_s* sqd_batch_t;
 
 /* ---------------------------------------------------------------- library ------------------ */
 const char* sqd_version(void);
@@ -150,6 +151,10 @@ int sqd_grad_terms(sqd_op_t op, const void* u, const void* v, int dtype, double*
 /* Recomputes the cached matrix elements (cache z = 2) after sqd_paulis_set_coeffs; the
  * connectivity is unchanged. */
 int sqd_op_refresh(sqd_op_t op, void* stream);
+/* Frees the per-pair group indices of an operator with cached matrix elements (cache (1, 2)),
+ * 4 bytes per stored pair; the matvec, LOCG and batching keep working, while sqd_grad_terms,
+ * sqd_op_csr and sqd_op_refresh then return SQD_ERR_INVALID.  No rqutils counterpart. */
+int sqd_op_release_groups(sqd_op_t op);
 void sqd_op_destroy(sqd_op_t op);
 
 /* ---------------------------------------------------------------- LOCG --------------------- */
@@ -177,6 +182,23 @@ int sqd_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xini
              int64_t xinit_index, const void* const* orth, int n_orth, double tol, int maxiter,
              int mode, int use_graph, void* stream, double* eigval_host, void* eigvec,
              int* niter_host, double* residual_host);
+
+/* ---------------------------------------------------------------- batched instances -------- */
+/* Many independent SQD problems solved together (no rqutils counterpart: rqutils solves one
+ * subspace per call).  The operators' stored pairs (cache_strategy (1, 2) required) are copied
+ * into one block-diagonal operator; the operators may be destroyed afterwards. */
+int sqd_batch_create(const sqd_op_t* ops, int n_ops, void* stream, sqd_batch_t* out);
+int sqd_batch_info(sqd_batch_t b, int64_t* total_rows, int64_t* total_pairs);
+int sqd_batch_set_lanes(sqd_batch_t b, int precision, int lanes_per_row);
+/* Mixed-precision LOCG (as SQD_LOCG_MIXED of sqd_locg) for every instance at once: FP32 sweeps
+ * then FP64 iterations until each instance meets the reference's residual test with `tol`
+ * (< 0: dtype epsilon).  Start vectors: xinit (device, concatenated, dtype) or, if NULL,
+ * one-hot vectors at xinit_index_host[i] (local row of instance i).  Outputs per instance:
+ * eigvals_host[n], niters_host[n], residuals_host[n] (may be NULL); eigvecs concatenated. */
+int sqd_batch_locg(sqd_batch_t b, int dtype, const void* xinit, const int64_t* xinit_index_host,
+                   double tol, int maxiter, int use_graph, void* stream, double* eigvals_host,
+                   void* eigvecs, int* niters_host, double* residuals_host);
+void sqd_batch_destroy(sqd_batch_t b);
 
 #ifdef __cplusplus
 }

@@ -66,6 +66,13 @@ EXTRA_PROTOTYPES = {
     'sqd_trim_memory': (_i32, [_u64]),
     'sqd_paulis_set_coeffs': (_i32, [_vp, _vp, _vp, _vp, _c.POINTER(_i32)]),
     'sqd_op_refresh': (_i32, [_vp, _vp]),
+    'sqd_batch_create': (_i32, [_c.POINTER(_vp), _i32, _vp, _c.POINTER(_vp)]),
+    'sqd_batch_info': (_i32, [_vp, _c.POINTER(_i64), _c.POINTER(_i64)]),
+    'sqd_batch_set_lanes': (_i32, [_vp, _i32, _i32]),
+    'sqd_batch_locg': (_i32, [_vp, _i32, _vp, _c.POINTER(_i64), _f64, _i32, _i32, _vp,
+                              _c.POINTER(_f64), _vp, _c.POINTER(_i32), _c.POINTER(_f64)]),
+    'sqd_batch_destroy': (None, [_vp]),
+    'sqd_op_release_groups': (_i32, [_vp]),
 }
 
 

@@ -17,6 +17,7 @@
 
 #include "internal.cuh"
 #include "dispatch.cuh"
+#include "accum.cuh"
 
 namespace sqd {
 namespace {
@@ -1046,6 +1047,537 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xin
 }  // namespace
 }  // namespace sqd
 
+// ============================================================================================
+// Batched instances: many independent operators solved together.
+//
+// The instances' stored pairs are concatenated into one block-diagonal CSR.  Rows are cut
+// into tiles that never cross an instance boundary; every kernel walks the tile list (a
+// per-instance work queue) and skips the tiles of instances that have converged.  Inner
+// products are reduced per tile and then per instance (one warp per instance, tiles in fixed
+// order, so results are deterministic), after which that warp runs the instance's scalar step
+// (Rayleigh-Ritz, normalisations, convergence) on its own coefficient bank.  A whole batched
+// iteration is one CUDA graph body; the WHILE condition is "some instance still active".
+// ============================================================================================
+struct sqd_batch_s {
+  int n = 0;
+  int value_complex = 0;
+  int64_t total_rows = 0;
+  int64_t total_nnz = 0;
+  std::vector<int64_t> row0;          // host [n + 1]
+  sqd::DevBuf<int64_t> row_ptr;       // [total_rows + 1]
+  sqd::DevBuf<uint32_t> cols;         // [total_nnz] global source rows
+  sqd::DevBuf<double> values;         // [total_nnz * nca]
+  sqd::DevBuf<float> values32;        // FP32 copy
+  int n_tiles = 0;
+  sqd::DevBuf<int32_t> tile_inst;     // [n_tiles]
+  sqd::DevBuf<int64_t> tile_row0;     // [n_tiles + 1]
+  std::vector<int32_t> inst_tile0;    // host [n + 1]
+  sqd::DevBuf<int32_t> inst_tile0_d;  // [n + 1]
+  int lanes[2] = {8, 8};
+};
+
+namespace sqd {
+namespace {
+
+constexpr int64_t kTileRows = 2048;
+
+template <typename R, int NCV, int NCA, int LPR>
+__global__ void __launch_bounds__(256)
+k_bmv_csr(const int64_t* __restrict__ row_ptr, const uint32_t* __restrict__ cols,
+          const R* __restrict__ vals, const R* __restrict__ v, R* __restrict__ out,
+          const int32_t* __restrict__ tile_inst, const int64_t* __restrict__ tile_row0,
+          int n_tiles, const LocgDev* dev) {
+  constexpr int RPW = 32 / LPR;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sub = lane % LPR, slot = lane / LPR;
+  const int nwarps = blockDim.x >> 5;
+  for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    if (*(volatile const int*)&dev[tile_inst[t]].done) continue;
+    const int64_t r0 = tile_row0[t], r1 = tile_row0[t + 1];
+    for (int64_t rb = r0 + int64_t(warp) * RPW; rb < r1; rb += int64_t(nwarps) * RPW) {
+      const int64_t row = rb + slot;
+      CAcc<R, NCV, NCA> acc;
+      if (row < r1) {
+        const int64_t b = __ldg(row_ptr + row), e = __ldg(row_ptr + row + 1);
+        for (int64_t i = b + sub; i < e; i += LPR)
+          acc.add(ld_elem<R, NCA>(vals, i), ld_elem<R, NCV>(v, __ldg(cols + i)));
+      }
+      acc.merge(LPR);
+      if (sub == 0 && row < r1)
+        st_elem<R, NCV>(out, row, cx_make<R>(acc.re.value(), acc.im.value()));
+    }
+  }
+}
+
+template <int MAXS, int MAXD, int MAXO>
+struct BLCArgs {
+  const void* src[MAXS];
+  void* out[MAXO];
+  int nsrc, nout, ndot, gate;
+  signed char da[MAXD], db[MAXD];
+  LocgDev* dev;
+  double* partials;
+  const int32_t* tile_inst;
+  const int64_t* tile_row0;
+  int n_tiles;
+};
+
+template <typename R, int NC, int MAXS, int MAXD, int MAXO>
+__global__ void __launch_bounds__(LC_THREADS) k_blc(BLCArgs<MAXS, MAXD, MAXO> a) {
+  __shared__ double2 sc[MAXO][MAXS];
+  __shared__ double sred[MAXD * 2][LC_THREADS / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
+    const LocgDev* dev = a.dev + a.tile_inst[t];
+    __syncthreads();
+    const bool skip = ((a.gate & G_DONE) && *(volatile const int*)&dev->done) ||
+                      ((a.gate & G_KEEP) && *(volatile const int*)&dev->keep);
+    if (skip) {
+      if (threadIdx.x < 2 * a.ndot)
+        a.partials[static_cast<int64_t>(t) * (2 * MAXD) + threadIdx.x] = 0.0;
+      continue;
+    }
+    for (int q = threadIdx.x; q < MAXO * MAXS; q += blockDim.x)
+      sc[q / MAXS][q % MAXS] = make_double2(dev->coef[q / MAXS][q % MAXS][0],
+                                            dev->coef[q / MAXS][q % MAXS][1]);
+    __syncthreads();
+    double acc[MAXD][2];
+#pragma unroll
+    for (int d = 0; d < MAXD; ++d) acc[d][0] = acc[d][1] = 0.0;
+    const int64_t e = a.tile_row0[t + 1];
+    for (int64_t i = a.tile_row0[t] + threadIdx.x; i < e; i += blockDim.x) {
+      double2 s[MAXS];
+#pragma unroll
+      for (int k = 0; k < MAXS; ++k) {
+        s[k] = make_double2(0.0, 0.0);
+        if (k < a.nsrc) {
+          const Cx<R> v = ld_elem_rw<R, NC>(static_cast<const R*>(a.src[k]), i);
+          s[k] = make_double2(double(v.re), double(v.im));
+        }
+      }
+      double2 o[MAXO];
+#pragma unroll
+      for (int q = 0; q < MAXO; ++q) {
+        o[q] = make_double2(0.0, 0.0);
+        if (q < a.nout) {
+#pragma unroll
+          for (int k = 0; k < MAXS; ++k)
+            if (k < a.nsrc) o[q] = cadd(o[q], cmul(sc[q][k], s[k]));
+          if constexpr (NC == 1) o[q].y = 0.0;
+        }
+      }
+#pragma unroll
+      for (int d = 0; d < MAXD; ++d) {
+        if (d < a.ndot) {
+          double2 x = make_double2(0.0, 0.0), y = make_double2(0.0, 0.0);
+          const int ca = a.da[d], cb = a.db[d];
+#pragma unroll
+          for (int k = 0; k < MAXS; ++k) {
+            if (ca == k) x = s[k];
+            if (cb == k) y = s[k];
+          }
+#pragma unroll
+          for (int q = 0; q < MAXO; ++q) {
+            if (ca == 100 + q) x = o[q];
+            if (cb == 100 + q) y = o[q];
+          }
+          acc[d][0] += x.x * y.x + x.y * y.y;
+          acc[d][1] += x.x * y.y - x.y * y.x;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < MAXO; ++q)
+        if (q < a.nout && a.out[q] != nullptr)
+          st_elem<R, NC>(static_cast<R*>(a.out[q]), i, cx_make<R>(R(o[q].x), R(o[q].y)));
+    }
+    if (a.ndot > 0) {
+#pragma unroll
+      for (int d = 0; d < MAXD; ++d) {
+        if (d < a.ndot) {
+          const double v0 = warp_sum(acc[d][0]);
+          const double v1 = warp_sum(acc[d][1]);
+          if (lane == 0) {
+            sred[2 * d][warp] = v0;
+            sred[2 * d + 1][warp] = v1;
+          }
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x < 2 * a.ndot) {
+        double v = 0.0;
+        for (int w = 0; w < LC_THREADS / 32; ++w) v += sred[threadIdx.x][w];
+        a.partials[static_cast<int64_t>(t) * (2 * MAXD) + threadIdx.x] = v;
+      }
+    }
+  }
+}
+
+// One warp per instance: sum its tiles' partials in order, then run its scalar step.
+__global__ void k_bpost(const double* partials, int stride, const int32_t* inst_tile0, int n,
+                        LocgDev* dev, int ndot, int nsrc, int post, int gate) {
+  const int inst = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (inst >= n) return;
+  LocgDev* d = dev + inst;
+  if ((gate & G_DONE) && d->done) return;
+  if (lane < 2 * ndot) {
+    double v = 0.0;
+    for (int t = inst_tile0[inst]; t < inst_tile0[inst + 1]; ++t)
+      v += partials[static_cast<int64_t>(t) * stride + lane];
+    d->red[lane >> 1][lane & 1] = v;
+  }
+  __syncwarp();
+  if (lane == 0) run_post(d, post, nsrc, 0, 0);
+}
+
+// Counts the active instances and sets the WHILE condition.
+__global__ void k_bactive(const LocgDev* dev, int n, int use_cond,
+                          cudaGraphConditionalHandle cond, int* active) {
+  __shared__ int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  int c = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) c += dev[i].done ? 0 : 1;
+  atomicAdd(&cnt, c);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *active = cnt;
+    if (use_cond) cudaGraphSetConditional(cond, cnt > 0 ? 1u : 0u);
+  }
+}
+
+template <typename R, int NC>
+__global__ void k_bonehot(R* x, const int32_t* tile_inst, const int64_t* tile_row0, int n_tiles,
+                          const int64_t* row0, const int64_t* idx) {
+  for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    const int inst = tile_inst[t];
+    const int64_t hot = row0[inst] + idx[inst];
+    for (int64_t i = tile_row0[t] + threadIdx.x; i < tile_row0[t + 1]; i += blockDim.x)
+      st_elem<R, NC>(x, i, cx_make<R>(R(i == hot ? 1 : 0), R(0)));
+  }
+}
+
+template <typename R, int NC>
+class BLocg {
+ public:
+  using Tiny = BLCArgs<3, 3, 2>;
+  using Wide = BLCArgs<6, 10, 5>;
+
+  BLocg(sqd_batch_s* b, cudaStream_t st) : b_(b), st_(st), cur_(st) {
+    const int64_t n = b->total_rows;
+    for (auto* v : {&x_, &y_, &r_, &p_, &ax_, &ay_, &ap_}) v->alloc(static_cast<size_t>(n) * NC, st);
+    dev_.alloc(b->n, st);
+    partials_.alloc(static_cast<size_t>(b->n_tiles) * 20, st);
+    active_.alloc(1, st);
+    SQD_CUDA(cudaMemsetAsync(dev_.ptr, 0, sizeof(LocgDev) * b->n, st));
+    SQD_CUDA(cudaMallocHost(reinterpret_cast<void**>(&host_), sizeof(LocgDev) * b->n));
+    blocks_ = static_cast<unsigned>(std::max(1, std::min(b->n_tiles, 8 * num_sms())));
+  }
+  ~BLocg() {
+    if (exec_) cudaGraphExecDestroy(exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    if (host_) cudaFreeHost(host_);
+  }
+  R* x() { return x_.ptr; }
+  const LocgDev& host(int i) const { return host_[i]; }
+
+  void set_params(double tol, int maxiter, double inner_rtol, double etol, int stall) {
+    std::vector<LocgDev> h(b_->n);
+    for (int i = 0; i < b_->n; ++i) {
+      h[i] = LocgDev{};
+      h[i].tol = tol;
+      h[i].nscale = 10.0 * static_cast<double>(b_->row0[i + 1] - b_->row0[i]);
+      h[i].maxiter = maxiter;
+      h[i].inner_rtol = inner_rtol;
+      h[i].etol = etol;
+      h[i].stall = stall;
+      h[i].best_r = 1e300;
+    }
+    SQD_CUDA(cudaMemcpyAsync(dev_.ptr, h.data(), sizeof(LocgDev) * b_->n,
+                             cudaMemcpyHostToDevice, st_));
+    SQD_CUDA(cudaStreamSynchronize(st_));
+  }
+
+  void lc(std::initializer_list<const void*> srcs, std::initializer_list<void*> outs,
+          std::initializer_list<std::pair<int, int>> dots, int post, int gate = G_NONE) {
+    if (srcs.size() <= 3 && dots.size() <= 3 && outs.size() <= 2) {
+      Tiny a{};
+      fill(a, srcs, outs, dots, gate);
+      if (srcs.size() > 0) k_blc<R, NC, 3, 3, 2><<<blocks_, LC_THREADS, 0, cur_>>>(a);
+      SQD_CHECK_LAUNCH();
+      posts(a.nsrc, static_cast<int>(dots.size()), 6, post, gate);
+    } else {
+      SQD_REQUIRE(srcs.size() <= 6 && dots.size() <= 10 && outs.size() <= 5, "pass too wide");
+      Wide a{};
+      fill(a, srcs, outs, dots, gate);
+      k_blc<R, NC, 6, 10, 5><<<blocks_, LC_THREADS, 0, cur_>>>(a);
+      SQD_CHECK_LAUNCH();
+      posts(a.nsrc, static_cast<int>(dots.size()), 20, post, gate);
+    }
+  }
+  void post_only(int post, int gate = G_NONE) { posts(0, 0, 6, post, gate); }
+
+  void matvec(const R* in, R* out) {
+    const int prec = sizeof(R) == 8 ? 0 : 1;
+    const R* vals;
+    if constexpr (sizeof(R) == 8) vals = b_->values.ptr;
+    else vals = b_->values32.ptr;
+    auto launch = [&](auto nca_t) {
+      constexpr int NCA = decltype(nca_t)::value;
+      dispatch_lpr(b_->lanes[prec], [&](auto lpr_t) {
+        constexpr int LPR = decltype(lpr_t)::value;
+        const unsigned G = static_cast<unsigned>(std::max(1, std::min(b_->n_tiles, 16 * num_sms())));
+        k_bmv_csr<R, NC, NCA, LPR><<<G, 256, 0, cur_>>>(b_->row_ptr.ptr, b_->cols.ptr, vals, in,
+                                                        out, b_->tile_inst.ptr,
+                                                        b_->tile_row0.ptr, b_->n_tiles, dev_.ptr);
+      });
+    };
+    if constexpr (NC == 2) {
+      if (b_->value_complex) launch(IntTag<2>{});
+      else launch(IntTag<1>{});
+    } else {
+      launch(IntTag<1>{});
+    }
+    SQD_CHECK_LAUNCH();
+  }
+
+  void read_host() {
+    SQD_CUDA(cudaMemcpyAsync(host_, dev_.ptr, sizeof(LocgDev) * b_->n, cudaMemcpyDeviceToHost,
+                             st_));
+    SQD_CUDA(cudaStreamSynchronize(st_));
+  }
+  int active() {
+    int h = 0;
+    k_bactive<<<1, 256, 0, st_>>>(dev_.ptr, b_->n, 0, 0, active_.ptr);
+    SQD_CHECK_LAUNCH();
+    copy_to_host(&h, active_.ptr, 1, st_);
+    return h;
+  }
+
+  void onehot(const int64_t* idx_host) {
+    DevBuf<int64_t> row0, idx;
+    row0.alloc(b_->n + 1, st_);
+    idx.alloc(b_->n, st_);
+    SQD_CUDA(cudaMemcpyAsync(row0.ptr, b_->row0.data(), sizeof(int64_t) * (b_->n + 1),
+                             cudaMemcpyHostToDevice, st_));
+    SQD_CUDA(cudaMemcpyAsync(idx.ptr, idx_host, sizeof(int64_t) * b_->n, cudaMemcpyHostToDevice,
+                             st_));
+    k_bonehot<R, NC><<<blocks_, 256, 0, st_>>>(x_.ptr, b_->tile_inst.ptr, b_->tile_row0.ptr,
+                                               b_->n_tiles, row0.ptr, idx.ptr);
+    SQD_CHECK_LAUNCH();
+    SQD_CUDA(cudaStreamSynchronize(st_));
+  }
+
+  // Same sequence as Locg::start_implicit, every pass after the first residual gated so that
+  // instances whose start vector is exact stop there.
+  void start_implicit() {
+    R *x = x_.ptr, *y = y_.ptr, *r = r_.ptr, *p = p_.ptr, *ax = ax_.ptr, *ay = ay_.ptr,
+      *ap = ap_.ptr;
+    const int g = G_DONE;
+    lc({x}, {}, {{0, 0}}, P_INV_NORM);
+    lc({x}, {x}, {}, P_NONE);
+    matvec(x, ax);
+    lc({ax, x}, {}, {{1, 0}}, P_THETA0);
+    lc({ax, x}, {r}, {{100, 100}}, P_R0NORM);
+    SQD_CUDA(cudaMemsetAsync(y, 0, sizeof(R) * NC * b_->total_rows, cur_));
+    SQD_CUDA(cudaMemsetAsync(ay, 0, sizeof(R) * NC * b_->total_rows, cur_));
+    lc({r}, {p}, {}, P_NONE, g);
+    matvec(p, ap);
+    lc({x, p, ax, ap}, {}, {{0, 2}, {1, 2}, {1, 3}}, P_RR2, g);
+    lc({ax, ap}, {ay, ax}, {}, P_NONE, g);
+    lc({x, p}, {y, x}, {{100, 100}, {101, 101}}, P_TU_NORM, g);
+    lc({x, y}, {x, y}, {}, P_NONE, g);
+    lc({ax, ay}, {ax, ay}, {}, P_SET_R_COEF, g);
+    lc({ax, x}, {r}, {{100, 100}, {0, 0}}, P_CONV, g);
+    lc({r, x, y}, {}, {{1, 0}, {2, 0}}, P_PROJ_IPS, g);
+  }
+
+  void body_fast() {
+    R *x = x_.ptr, *y = y_.ptr, *r = r_.ptr, *p = p_.ptr, *ax = ax_.ptr, *ay = ay_.ptr,
+      *ap = ap_.ptr;
+    const int g = G_DONE;
+    lc({r, x, y}, {p}, {{100, 100}, {1, 100}, {2, 100}}, P_PROJ_NORM_IPS, g);
+    lc({p, x, y}, {p}, {}, P_NONE, g);
+    matvec(p, ap);
+    lc({x, y, p, ax, ay, ap}, {},
+       {{0, 3}, {1, 4}, {2, 5}, {1, 3}, {2, 3}, {2, 4}, {2, 2}, {1, 2}}, P_GRAM_IMPLICIT, g);
+    lc({x, y, p, ax, ay, ap}, {x, y, ax, ay}, {{100, 100}, {101, 101}}, P_UPDATE_NORMS, g);
+    lc({x, y, ax, ay}, {x, y, ax, ay, r}, {{104, 104}, {102, 102}, {100, 104}, {101, 104}},
+       P_CONV_PROJ, g);
+    k_bactive<<<1, 256, 0, cur_>>>(dev_.ptr, b_->n, use_cond_, cond_, active_.ptr);
+    SQD_CHECK_LAUNCH();
+  }
+
+  // Explicit A x, A y, residual and convergence test for every instance (drift check).
+  void refresh() {
+    post_only(P_RESET);
+    matvec(x_.ptr, ax_.ptr);
+    matvec(y_.ptr, ay_.ptr);
+    lc({ax_.ptr, x_.ptr}, {}, {{1, 0}}, P_THETA0);
+    lc({ax_.ptr, x_.ptr}, {r_.ptr}, {{100, 100}, {0, 0}}, P_CONV);
+    lc({r_.ptr, x_.ptr, y_.ptr}, {}, {{1, 0}, {2, 0}}, P_PROJ_IPS);
+  }
+
+  void loop(bool use_graph) {
+    if (active() == 0) return;
+    if (!use_graph) {
+      for (;;) {
+        body_fast();
+        if (active() == 0) break;
+      }
+      return;
+    }
+    if (!exec_) {
+      SQD_CUDA(cudaGraphCreate(&graph_, 0));
+      SQD_CUDA(cudaGraphConditionalHandleCreate(&cond_, graph_, 1, cudaGraphCondAssignDefault));
+      cudaGraphNodeParams cp{};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = cond_;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t node;
+      SQD_CUDA(cudaGraphAddNode(&node, graph_, nullptr, 0, &cp));
+      cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+      cudaStream_t cap = nullptr;
+      SQD_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+      cur_ = cap;
+      use_cond_ = 1;
+      auto restore = [&] {
+        cur_ = st_;
+        use_cond_ = 0;
+        cudaStreamDestroy(cap);
+      };
+      cudaError_t cerr = cudaStreamBeginCaptureToGraph(cap, bodyg, nullptr, nullptr, 0,
+                                                       cudaStreamCaptureModeThreadLocal);
+      if (cerr != cudaSuccess) {
+        restore();
+        SQD_CUDA(cerr);
+      }
+      try {
+        body_fast();
+      } catch (...) {
+        cudaGraph_t dummy;
+        cudaStreamEndCapture(cap, &dummy);
+        restore();
+        throw;
+      }
+      cerr = cudaStreamEndCapture(cap, &bodyg);
+      restore();
+      SQD_CUDA(cerr);
+      SQD_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
+    }
+    SQD_CUDA(cudaGraphLaunch(exec_, st_));
+    SQD_CUDA(cudaStreamSynchronize(st_));
+  }
+
+  DevBuf<R> x_, y_, r_, p_, ax_, ay_, ap_;
+
+ private:
+  template <typename A>
+  void fill(A& a, std::initializer_list<const void*> srcs, std::initializer_list<void*> outs,
+            std::initializer_list<std::pair<int, int>> dots, int gate) {
+    int k = 0;
+    for (auto s : srcs) a.src[k++] = s;
+    a.nsrc = k;
+    k = 0;
+    for (auto o : outs) a.out[k++] = o;
+    a.nout = k;
+    k = 0;
+    for (auto d : dots) {
+      a.da[k] = static_cast<signed char>(d.first);
+      a.db[k] = static_cast<signed char>(d.second);
+      ++k;
+    }
+    a.ndot = k;
+    a.gate = gate;
+    a.dev = dev_.ptr;
+    a.partials = partials_.ptr;
+    a.tile_inst = b_->tile_inst.ptr;
+    a.tile_row0 = b_->tile_row0.ptr;
+    a.n_tiles = b_->n_tiles;
+  }
+  void posts(int nsrc, int ndot, int stride, int post, int gate) {
+    if (post == P_NONE && ndot == 0) return;
+    const unsigned G = grid_for(static_cast<int64_t>(b_->n) * 32, 256);
+    k_bpost<<<G, 256, 0, cur_>>>(partials_.ptr, stride, b_->inst_tile0_d.ptr, b_->n, dev_.ptr,
+                                 ndot, nsrc, post, gate);
+    SQD_CHECK_LAUNCH();
+  }
+
+  sqd_batch_s* b_;
+  cudaStream_t st_, cur_;
+  unsigned blocks_ = 1;
+  DevBuf<LocgDev> dev_;
+  DevBuf<double> partials_;
+  DevBuf<int> active_;
+  LocgDev* host_ = nullptr;
+  int use_cond_ = 0;
+  cudaGraphConditionalHandle cond_ = 0;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t exec_ = nullptr;
+};
+
+template <int NC>
+void run_batch(sqd_batch_s* b, const double* xinit, const int64_t* xidx, double tol, int maxiter,
+               bool use_graph, cudaStream_t st, double* eig, double* vecs, int* niter,
+               double* resid) {
+  constexpr double kInnerRtol = 2e-7;
+  constexpr int kStall = 25;
+  constexpr int kRestarts = 6;
+  const double eps64 = 2.220446049250313e-16;
+  const int64_t n = b->total_rows;
+  const unsigned G = grid_for(n, 256, 8192);
+  std::vector<int> it32(b->n, 0);
+  DevBuf<double> x64;
+  x64.alloc(static_cast<size_t>(n) * NC, st);
+  {
+    BLocg<float, NC> L(b, st);
+    L.set_params(0.0, maxiter, kInnerRtol, 0.0, kStall);
+    if (xinit)
+      k_convert<float, double, NC><<<G, 256, 0, st>>>(xinit, L.x(), n);
+    else
+      L.onehot(xidx);
+    SQD_CHECK_LAUNCH();
+    L.start_implicit();
+    for (int k = 0; k < kRestarts; ++k) {
+      L.loop(use_graph);
+      L.refresh();
+      if (L.active() == 0) break;
+    }
+    L.read_host();
+    for (int i = 0; i < b->n; ++i) it32[i] = L.host(i).niter;
+    k_convert<double, float, NC><<<G, 256, 0, st>>>(L.x(), x64.ptr, n);
+    SQD_CHECK_LAUNCH();
+  }
+  BLocg<double, NC> L(b, st);
+  L.set_params(tol < 0 ? eps64 : tol, maxiter, 0.0, 0.0, 0);
+  SQD_CUDA(cudaMemcpyAsync(L.x(), x64.ptr, sizeof(double) * NC * n, cudaMemcpyDeviceToDevice, st));
+  L.start_implicit();
+  L.loop(use_graph);
+  L.read_host();
+  for (int i = 0; i < b->n; ++i) {
+    eig[i] = L.host(i).theta;
+    niter[i] = it32[i] + L.host(i).niter;
+    if (resid) resid[i] = L.host(i).rnorm;
+  }
+  SQD_CUDA(cudaMemcpyAsync(vecs, L.x(), sizeof(double) * NC * n, cudaMemcpyDeviceToDevice, st));
+  SQD_CUDA(cudaStreamSynchronize(st));
+}
+
+__global__ void k_add_i64(const int64_t* in, int64_t* out, int64_t n, int64_t add) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = in[i] + add;
+}
+__global__ void k_add_u32(const uint32_t* in, uint32_t* out, int64_t n, uint32_t add) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = in[i] + add;
+}
+
+}  // namespace
+}  // namespace sqd
+
 using namespace sqd;
 
 extern "C" int sqd_op_matvec_cb(void* ctx, const void* x, void* y, void* stream) {
@@ -1110,3 +1642,132 @@ extern "C" int sqd_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const
                   eigval_host, eigvec, niter_host, residual_host);
   });
 }
+
+// ---------------------------------------------------------------------------- batched C ABI
+extern "C" int sqd_batch_create(const sqd_op_t* ops, int n_ops, void* stream,
+                                sqd_batch_t* out) {
+  return guarded([&] {
+    SQD_REQUIRE(out != nullptr, "out handle is NULL");
+    *out = nullptr;
+    SQD_REQUIRE(ops != nullptr && n_ops >= 1, "no operators");
+    cudaStream_t st = as_stream(stream);
+    auto b = std::make_unique<sqd_batch_s>();
+    b->n = n_ops;
+    b->value_complex = ops[0]->value_complex;
+    b->row0.assign(n_ops + 1, 0);
+    std::vector<int64_t> nnz0(n_ops + 1, 0);
+    for (int i = 0; i < n_ops; ++i) {
+      const sqd_op_s* op = ops[i];
+      SQD_REQUIRE(op != nullptr, "NULL operator");
+      SQD_REQUIRE(op->x_cache == 1 && op->z_cache == 2,
+                  "batched operators need cache_strategy (1, 2)");
+      SQD_REQUIRE(op->value_complex == b->value_complex,
+                  "batched operators must all be real or all complex");
+      b->row0[i + 1] = b->row0[i] + op->s->states_size;
+      nnz0[i + 1] = nnz0[i] + op->nnz;
+    }
+    b->total_rows = b->row0[n_ops];
+    b->total_nnz = nnz0[n_ops];
+    SQD_REQUIRE(b->total_rows < (int64_t(1) << 32), "batch limited to 2^32 rows");
+    const int nca = b->value_complex ? 2 : 1;
+    b->row_ptr.alloc(b->total_rows + 1, st);
+    b->cols.alloc(std::max<int64_t>(b->total_nnz, 1), st);
+    b->values.alloc(std::max<int64_t>(b->total_nnz, 1) * nca, st);
+    for (int i = 0; i < n_ops; ++i) {
+      const sqd_op_s* op = ops[i];
+      const int64_t rows = op->s->states_size;
+      k_add_i64<<<grid_for(rows, 256, 4096), 256, 0, st>>>(op->row_ptr.ptr,
+                                                            b->row_ptr.ptr + b->row0[i], rows,
+                                                            nnz0[i]);
+      if (op->nnz > 0) {
+        k_add_u32<<<grid_for(op->nnz, 256, 8192), 256, 0, st>>>(
+            op->cols.ptr, b->cols.ptr + nnz0[i], op->nnz, static_cast<uint32_t>(b->row0[i]));
+        SQD_CUDA(cudaMemcpyAsync(b->values.ptr + nnz0[i] * nca, op->values.ptr,
+                                 sizeof(double) * op->nnz * nca, cudaMemcpyDeviceToDevice, st));
+      }
+      SQD_CHECK_LAUNCH();
+    }
+    SQD_CUDA(cudaMemcpyAsync(b->row_ptr.ptr + b->total_rows, &b->total_nnz, sizeof(int64_t),
+                             cudaMemcpyHostToDevice, st));
+    const size_t nv = static_cast<size_t>(std::max<int64_t>(b->total_nnz, 1)) * nca;
+    b->values32.alloc(nv, st);
+    k_convert<float, double, 1><<<grid_for(nv, 256, 16384), 256, 0, st>>>(b->values.ptr,
+                                                                         b->values32.ptr, nv);
+    SQD_CHECK_LAUNCH();
+    // tiles
+    std::vector<int32_t> ti;
+    std::vector<int64_t> tr;
+    b->inst_tile0.assign(n_ops + 1, 0);
+    for (int i = 0; i < n_ops; ++i) {
+      b->inst_tile0[i] = static_cast<int32_t>(ti.size());
+      for (int64_t r = b->row0[i]; r < b->row0[i + 1]; r += kTileRows) {
+        ti.push_back(i);
+        tr.push_back(r);
+      }
+    }
+    b->inst_tile0[n_ops] = static_cast<int32_t>(ti.size());
+    tr.push_back(b->total_rows);
+    b->n_tiles = static_cast<int>(ti.size());
+    b->tile_inst.alloc(ti.size(), st);
+    b->tile_row0.alloc(tr.size(), st);
+    b->inst_tile0_d.alloc(n_ops + 1, st);
+    SQD_CUDA(cudaMemcpyAsync(b->tile_inst.ptr, ti.data(), sizeof(int32_t) * ti.size(),
+                             cudaMemcpyHostToDevice, st));
+    SQD_CUDA(cudaMemcpyAsync(b->tile_row0.ptr, tr.data(), sizeof(int64_t) * tr.size(),
+                             cudaMemcpyHostToDevice, st));
+    SQD_CUDA(cudaMemcpyAsync(b->inst_tile0_d.ptr, b->inst_tile0.data(),
+                             sizeof(int32_t) * (n_ops + 1), cudaMemcpyHostToDevice, st));
+    const double avg = b->total_rows > 0 ? double(b->total_nnz) / double(b->total_rows) : 0.0;
+    const int lpr = avg >= 96 ? 32 : avg >= 40 ? 16 : avg >= 16 ? 8 : avg >= 6 ? 4 : 2;
+    b->lanes[0] = b->lanes[1] = lpr;
+    SQD_CUDA(cudaStreamSynchronize(st));
+    *out = b.release();
+  });
+}
+
+extern "C" int sqd_batch_info(sqd_batch_t b, int64_t* total_rows, int64_t* total_pairs) {
+  return guarded([&] {
+    SQD_REQUIRE(b != nullptr, "NULL batch");
+    if (total_rows) *total_rows = b->total_rows;
+    if (total_pairs) *total_pairs = b->total_nnz;
+  });
+}
+
+extern "C" int sqd_batch_set_lanes(sqd_batch_t b, int precision, int lanes_per_row) {
+  return guarded([&] {
+    SQD_REQUIRE(b != nullptr, "NULL batch");
+    SQD_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (FP32)");
+    dispatch_lpr(lanes_per_row, [](auto) {});
+    b->lanes[precision] = lanes_per_row;
+  });
+}
+
+extern "C" int sqd_batch_locg(sqd_batch_t b, int dtype, const void* xinit,
+                              const int64_t* xinit_index_host, double tol, int maxiter,
+                              int use_graph, void* stream, double* eigvals_host, void* eigvecs,
+                              int* niters_host, double* residuals_host) {
+  return guarded([&] {
+    SQD_REQUIRE(b != nullptr && eigvals_host && eigvecs && niters_host, "NULL argument");
+    SQD_REQUIRE(dtype == SQD_F64 || dtype == SQD_C128, "batched LOCG dtype must be F64 or C128");
+    SQD_REQUIRE(dtype == SQD_C128 || !b->value_complex,
+                "a complex Hamiltonian needs complex vectors");
+    SQD_REQUIRE(xinit != nullptr || xinit_index_host != nullptr, "no start vectors");
+    if (!xinit)
+      for (int i = 0; i < b->n; ++i)
+        SQD_REQUIRE(xinit_index_host[i] >= 0 &&
+                        xinit_index_host[i] < b->row0[i + 1] - b->row0[i],
+                    "start index out of range");
+    SQD_REQUIRE(maxiter >= 1, "maxiter must be positive");
+    cudaStream_t st = as_stream(stream);
+    if (dtype == SQD_C128)
+      run_batch<2>(b, static_cast<const double*>(xinit), xinit_index_host, tol, maxiter,
+                   use_graph != 0, st, eigvals_host, static_cast<double*>(eigvecs), niters_host,
+                   residuals_host);
+    else
+      run_batch<1>(b, static_cast<const double*>(xinit), xinit_index_host, tol, maxiter,
+                   use_graph != 0, st, eigvals_host, static_cast<double*>(eigvecs), niters_host,
+                   residuals_host);
+  });
+}
+
+extern "C" void sqd_batch_destroy(sqd_batch_t b) { delete b; }

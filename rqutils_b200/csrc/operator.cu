@@ -552,6 +552,8 @@ extern "C" int sqd_op_csr(sqd_op_t op, int64_t* indptr, int32_t* indices, double
   return guarded([&] {
     SQD_REQUIRE(op != nullptr, "NULL operator");
     SQD_REQUIRE(op->x_cache == 1, "CSR export needs cache_strategy x = 1");
+    SQD_REQUIRE(op->nnz == 0 || op->grps.ptr != nullptr,
+                "the operator released its group indices; create a new operator");
     sqd_paulis_s* p = op->p;
     sqd_space_s* sp = op->s;
     cudaStream_t st = as_stream(stream);
@@ -579,9 +581,20 @@ extern "C" int sqd_op_csr(sqd_op_t op, int64_t* indptr, int32_t* indices, double
   });
 }
 
+extern "C" int sqd_op_release_groups(sqd_op_t op) {
+  return guarded([&] {
+    SQD_REQUIRE(op != nullptr, "NULL operator");
+    SQD_REQUIRE(op->x_cache == 1 && op->z_cache == 2,
+                "only operators with cached matrix elements can release their group indices");
+    op->grps.release();
+  });
+}
+
 extern "C" int sqd_op_refresh(sqd_op_t op, void* stream) {
   return guarded([&] {
     SQD_REQUIRE(op != nullptr, "NULL operator");
+    SQD_REQUIRE(op->z_cache != 2 || op->nnz == 0 || op->grps.ptr != nullptr,
+                "the operator released its group indices; create a new operator");
     sqd_paulis_s* p = op->p;
     sqd_space_s* sp = op->s;
     SQD_REQUIRE(p->is_complex == op->value_complex,
@@ -614,6 +627,8 @@ extern "C" int sqd_grad_terms(sqd_op_t op, const void* u, const void* v, int dty
   return guarded([&] {
     SQD_REQUIRE(op != nullptr && u && v && out_terms, "NULL argument");
     SQD_REQUIRE(op->x_cache == 1, "the coefficient gradient needs cache_strategy x = 1");
+    SQD_REQUIRE(op->nnz == 0 || op->grps.ptr != nullptr,
+                "the operator released its group indices; create a new operator");
     SQD_REQUIRE(dtype == SQD_F64 || dtype == SQD_C128, "gradient dtype must be F64 or C128");
     SQD_REQUIRE(dtype == SQD_C128 || !op->value_complex, "complex Hamiltonian needs C128");
     sqd_paulis_s* p = op->p;

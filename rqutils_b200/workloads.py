@@ -234,6 +234,103 @@ def jw_hamiltonian(h1, h2, cutoff=1e-12):
     return x[keep], z[keep], re[keep]
 
 
+class JWStructure:
+    """The Pauli terms of ``jw_hamiltonian`` for ``norb`` orbitals and the linear map from the
+    independent integrals (h1 upper triangle, h2 canonical quadruples) to their coefficients,
+    so that many instances with different integrals cost one sparse matvec each."""
+
+    def __init__(self, norb):
+        from scipy.sparse import coo_matrix
+        self.norb = norb
+        nq = 2 * norb
+        idx1 = np.full((norb, norb), -1, dtype=np.int64)
+        k = 0
+        for i in range(norb):
+            for j in range(i, norb):
+                idx1[i, j] = idx1[j, i] = k
+                k += 1
+        self.n1 = k
+        ii, jj, kk, ll = np.meshgrid(*(np.arange(norb),) * 4, indexing='ij')
+        i0, j0 = np.minimum(ii, jj), np.maximum(ii, jj)
+        k0, l0 = np.minimum(kk, ll), np.maximum(kk, ll)
+        first = (i0 < k0) | ((i0 == k0) & (j0 <= l0))
+        key = np.stack([np.where(first, i0, k0), np.where(first, j0, l0),
+                        np.where(first, k0, i0), np.where(first, l0, j0)], axis=-1)
+        flat = ((key[..., 0] * norb + key[..., 1]) * norb + key[..., 2]) * norb + key[..., 3]
+        uniq, inv = np.unique(flat.ravel(), return_inverse=True)
+        self.h2_keys = uniq
+        self.idx2 = inv.reshape((norb,) * 4) + self.n1
+        self.nparam = self.n1 + uniq.shape[0]
+        xs, zs, res, ims, cols = [], [], [], [], []
+        i, j, s = (a.ravel() for a in np.meshgrid(np.arange(norb), np.arange(norb),
+                                                  np.arange(2), indexing='ij'))
+        part = _ladder_products([(i + norb * s, True), (j + norb * s, False)],
+                                np.ones(i.shape[0]), nq)
+        reps = 4
+        xs.append(part[0]); zs.append(part[1]); res.append(part[2]); ims.append(part[3])
+        cols.append(np.tile(idx1[i, j], reps))
+        i, j, k, l, s, t = (a.ravel() for a in np.meshgrid(*(np.arange(norb),) * 4, np.arange(2),
+                                                           np.arange(2), indexing='ij'))
+        p, q, r, u = i + norb * s, k + norb * t, l + norb * t, j + norb * s
+        keep = (p != q) & (r != u)
+        sel = np.nonzero(keep)[0]
+        chunk = 1 << 17
+        for a0 in range(0, sel.shape[0], chunk):
+            sl = sel[a0:a0 + chunk]
+            part = _ladder_products([(p[sl], True), (q[sl], True), (r[sl], False), (u[sl], False)],
+                                    np.full(sl.shape[0], 0.5), nq)
+            xs.append(part[0]); zs.append(part[1]); res.append(part[2]); ims.append(part[3])
+            cols.append(np.tile(self.idx2[i[sl], j[sl], k[sl], l[sl]], 16))
+        x = np.concatenate(xs)
+        z = np.concatenate(zs)
+        re = np.concatenate(res)
+        im = np.concatenate(ims)
+        col = np.concatenate(cols)
+        order = np.lexsort((z, x))
+        x, z = x[order], z[order]
+        new = np.concatenate([[True], (x[1:] != x[:-1]) | (z[1:] != z[:-1])])
+        row = np.cumsum(new) - 1
+        nterm = int(row[-1]) + 1
+        a_re = coo_matrix((re[order], (row, col[order])), shape=(nterm, self.nparam)).tocsr()
+        a_im = coo_matrix((im[order], (row, col[order])), shape=(nterm, self.nparam)).tocsr()
+        a_re.sum_duplicates()
+        a_im.sum_duplicates()
+        a_re.eliminate_zeros()
+        if a_im.nnz:
+            a_im.data[np.abs(a_im.data) < 1e-14] = 0.0
+            a_im.eliminate_zeros()
+        if a_im.nnz:
+            raise RuntimeError('JW map has imaginary coefficients')
+        a_re.data[np.abs(a_re.data) < 1e-15] = 0.0
+        a_re.eliminate_zeros()
+        live = np.diff(a_re.indptr) > 0
+        self.x = x[new][live]
+        self.z = z[new][live]
+        self.map = a_re[live]
+
+    def params(self, h1, h2):
+        p = np.zeros(self.nparam)
+        iu = np.triu_indices(self.norb)
+        idx = np.full((self.norb, self.norb), -1)
+        k = 0
+        for i, j in zip(*iu):
+            p[k] = h1[i, j]
+            k += 1
+        keys = self.h2_keys
+        n = self.norb
+        a, rem = np.divmod(keys, n ** 3)
+        b, rem = np.divmod(rem, n ** 2)
+        c, d = np.divmod(rem, n)
+        p[self.n1:] = h2[a, b, c, d]
+        return p
+
+    def hamiltonian(self, h1, h2, cutoff=1e-12):
+        """(x, z, coeff) of jw_hamiltonian(h1, h2) for symmetric h1 and 8-fold symmetric h2."""
+        c = self.map @ self.params(h1, h2)
+        keep = np.abs(c) > cutoff
+        return self.x[keep], self.z[keep], c[keep]
+
+
 # ---------------------------------------------------------------------------------------------
 # Standard workloads
 # ---------------------------------------------------------------------------------------------
@@ -270,10 +367,13 @@ def c1(seed=0):
     return Workload('c1', 16, x, z, c, states, seed, {'tol': 1e-10})
 
 
-def jw_workload(name, norb, nelec, na, nb, seed):
+def jw_workload(name, norb, nelec, na, nb, seed, structure=None):
     rng = np.random.default_rng(seed)
     h1, h2 = random_integrals(norb, rng)
-    x, z, c = jw_hamiltonian(h1, h2)
+    if structure is not None:
+        x, z, c = structure.hamiltonian(h1, h2)
+    else:
+        x, z, c = jw_hamiltonian(h1, h2)
     states = product_subspace(norb, nelec, na, nb, rng)
     return Workload(name, 2 * norb, x, z, c, states, seed, {'norb': norb, 'nelec': nelec,
                                                              'na': na, 'nb': nb})
@@ -300,10 +400,14 @@ def c4_dims(seed=0, count=96):
     return a, b
 
 
-def c4(seed=0, count=96):
+def c4(seed=0, count=96, structure=None):
+    """The batched workload: ``count`` 16-orbital JW instances with their own seeds (own
+    integrals and subspaces).  The Pauli terms are shared, so the coefficients come from one
+    ``JWStructure`` (built once, or passed in)."""
     a, b = c4_dims(seed, count)
-    return [jw_workload(f'c4_{i}', 16, 4, int(a[i]), int(b[i]), seed * 1000 + 101 + i)
-            for i in range(count)]
+    structure = structure or JWStructure(16)
+    return [jw_workload(f'c4_{i}', 16, 4, int(a[i]), int(b[i]), seed * 1000 + 101 + i,
+                        structure) for i in range(count)]
 
 
 def c5(seed=0, m=20000, d=1 << 20):
