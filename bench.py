@@ -39,7 +39,7 @@ def parse():
     ap.add_argument('--steps', type=int, default=20)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--workload', default='c2', choices=['c1', 'c2', 'c3', 'c5'])
+    ap.add_argument('--workload', default='c2', choices=['c1', 'c2', 'c3', 'c4', 'c5'])
     ap.add_argument('--cache', default='1,2')
     ap.add_argument('--no-locg', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
@@ -425,10 +425,70 @@ def locg_times(rq, op, wl, dev):
     return res
 
 
+def run_batched(args):
+    """C4: 96 16-orbital JW instances (own seeds, a_i x b_i product subspaces).  Times the
+    sequential per-instance FP64 solver loop and the batched mixed-precision solver, each from
+    operator construction to energies, and reports instances/s."""
+    import torch
+    torch.cuda.set_device(0)
+    import rqutils_b200 as rq
+    from rqutils_b200 import workloads as W, _lib
+    from rqutils_b200.batched import solve_instances
+    t0 = time.perf_counter()
+    structure = W.JWStructure(16)
+    instances = W.c4(0, structure=structure)
+    gen_s = time.perf_counter() - t0
+    count = len(instances)
+
+    def seq_fp64():
+        e = np.zeros(count)
+        it = np.zeros(count, dtype=np.int64)
+        for i, w in enumerate(instances):
+            ham = rq.PauliSumXZ.from_xz(w.x, w.z, w.coeffs, 32, force_real=True, padded=True)
+            op = rq.SQDOperator(ham, rq.Subspace.from_u64(w.states, 32), cache_strategy=(1, 2))
+            e[i], _, it[i] = rq.ground_locg(op, op.vinit(), vspace=(op.size, torch.complex128))
+            big = op.nnz > 1e9
+            del op, ham
+            if big:
+                _lib.trim_memory()
+        return e, it
+
+    res = {}
+    for name, fn in (('batched_mixed', lambda: solve_instances(instances)),
+                     ('sequential_fp64', seq_fp64)):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        e, it = fn()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t
+        _lib.trim_memory()
+        res[name] = {'time_s': dt, 'instances_per_s': count / dt, 'eigvals': e.tolist(),
+                     'niter_total': int(it.sum())}
+    e_b = np.array(res['batched_mixed']['eigvals'])
+    e_s = np.array(res['sequential_fp64']['eigvals'])
+    rel = np.abs(e_b - e_s) / np.abs(e_s)
+    a, b = W.c4_dims(0)
+    line = {'metric': 'C4 instances/s (96 JW instances, batched mixed vs sequential FP64)',
+            'value': res['batched_mixed']['instances_per_s'], 'unit': 'instances/s',
+            'higher_is_better': True, 'n_gpus': 1, 'dtype': 'complex128 results',
+            'data': 'synthetic (seeded generator)',
+            'config': {'workload': 'c4: 96 x (16-orbital JW, a_i x b_i 4-electron strings)',
+                       'rows_total': int(sum(w.states.shape[0] for w in instances)),
+                       'a': a.tolist(), 'b': b.tolist(), 'generation_s': gen_s},
+            'sequential_fp64': {k: v for k, v in res['sequential_fp64'].items()
+                                if k != 'eigvals'},
+            'batched_mixed': {k: v for k, v in res['batched_mixed'].items() if k != 'eigvals'},
+            'speedup': res['sequential_fp64']['time_s'] / res['batched_mixed']['time_s'],
+            'max_rel_energy_diff': float(rel.max()), 'median_rel_energy_diff': float(np.median(rel))}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == 'reference':
         run_reference(args)
+    elif args.workload == 'c4':
+        run_batched(args)
     else:
         run_ours(args)
 

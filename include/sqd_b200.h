@@ -123,6 +123,10 @@ int sqd_op_info(sqd_op_t op, int64_t* nnz, int64_t* states_size, int* value_comp
  * from the mean row length at creation; the autotuner overrides it. */
 int sqd_op_set_lanes(sqd_op_t op, int precision, int lanes_per_row);
 int sqd_op_get_lanes(sqd_op_t op, int precision, int* lanes_per_row);
+/* Second knob of the cached matvec: 0 = consecutive warps of the grid take consecutive rows;
+ * > 0 = each thread block owns chunk_rows consecutive rows at a time (L1 reuse of the source
+ * amplitudes that neighbouring rows share). */
+int sqd_op_set_chunk(sqd_op_t op, int precision, int64_t chunk_rows);
 /* Hv on the subspace (apply_h_x_cached and friends, sqd.py:643-743 via
  * make_x_cached_matvec sqd.py:746-751).  v and out have states_size elements of dtype. */
 int sqd_matvec(sqd_op_t op, const void* v, void* out, int dtype, void* stream);

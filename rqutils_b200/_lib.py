@@ -73,6 +73,7 @@ EXTRA_PROTOTYPES = {
                               _c.POINTER(_f64), _vp, _c.POINTER(_i32), _c.POINTER(_f64)]),
     'sqd_batch_destroy': (None, [_vp]),
     'sqd_op_release_groups': (_i32, [_vp]),
+    'sqd_op_set_chunk': (_i32, [_vp, _i32, _i64]),
 }
 
 

@@ -24,7 +24,9 @@ def _time(fn, reps):
     return e0.elapsed_time(e1) / reps
 
 
-def tune_lanes(op, dtype, candidates=(2, 4, 8, 16, 32), reps=5):
+def tune_lanes(op, dtype, candidates=(2, 4, 8, 16, 32), reps=5, chunks=(0, 64, 256, 1024)):
+    """Times every (lanes per row, chunk rows) schedule of the cached matvec for the precision
+    of ``dtype`` and keeps the fastest."""
     if op.cache_strategy[0] != 1:
         return {'lanes_per_row': None, 'note': 'uncached matvec has a fixed schedule'}
     if op.value_complex and not dtype.is_complex:
@@ -33,16 +35,23 @@ def tune_lanes(op, dtype, candidates=(2, 4, 8, 16, 32), reps=5):
     key = (op.size, op.nnz, op.cache_strategy, dtype)
     if key in _CACHE:
         op.set_lanes(precision, _CACHE[key]['lanes_per_row'])
+        op.set_chunk(precision, _CACHE[key]['chunk_rows'])
         return _CACHE[key]
     v = torch.randn(op.size, dtype=dtype, device=op.space.device)
     out = torch.empty_like(v)
     times = {}
-    for lpr in candidates:
-        op.set_lanes(precision, lpr)
-        times[lpr] = _time(lambda: op.matvec(v, out), reps)
+    for ch in chunks:
+        if ch and op.cache_strategy[1] != 2:
+            continue                       # the chunked schedule is a CSR-kernel option
+        op.set_chunk(precision, ch)
+        for lpr in candidates:
+            op.set_lanes(precision, lpr)
+            times[(lpr, ch)] = _time(lambda: op.matvec(v, out), reps)
     best = min(times, key=times.get)
-    op.set_lanes(precision, best)
-    res = {'lanes_per_row': best, 'ms': {str(k): round(t, 4) for k, t in times.items()}}
+    op.set_lanes(precision, best[0])
+    op.set_chunk(precision, best[1])
+    res = {'lanes_per_row': best[0], 'chunk_rows': best[1],
+           'ms': {f'{k[0]}/{k[1]}': round(t, 4) for k, t in times.items()}}
     _CACHE[key] = res
     return res
 

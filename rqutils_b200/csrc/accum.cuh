@@ -58,4 +58,28 @@ struct CAcc {
   }
 };
 
+// One lane's share of a CSR row: pairs i0, i0 + LPR, ... below e.  Four pairs per step with
+// independent index -> amplitude gathers in flight, then the remainder.
+template <typename R, int NCV, int NCA, int LPR>
+__device__ __forceinline__ void csr_row_dot(const uint32_t* __restrict__ cols,
+                                            const R* __restrict__ vals,
+                                            const R* __restrict__ v, int64_t i0, int64_t e,
+                                            CAcc<R, NCV, NCA>& acc) {
+  int64_t i = i0;
+  for (; i + 3 * LPR < e; i += 4 * LPR) {
+    uint32_t c[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) c[u] = __ldg(cols + i + u * LPR);
+    Cx<R> a[4], x[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a[u] = ld_elem<R, NCA>(vals, i + u * LPR);
+      x[u] = ld_elem<R, NCV>(v, c[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) acc.add(a[u], x[u]);
+  }
+  for (; i < e; i += LPR) acc.add(ld_elem<R, NCA>(vals, i), ld_elem<R, NCV>(v, __ldg(cols + i)));
+}
+
 }  // namespace sqd

@@ -65,6 +65,7 @@ struct sqd_op_s {
   int value_complex = 0;
   int64_t nnz = 0;
   int lanes_per_row[2] = {32, 32};  // [0]: FP64 vectors, [1]: FP32 vectors
+  int64_t chunk_rows[2] = {0, 0};   // rows a block owns at a time (0 = interleaved rows)
   sqd::DevBuf<int64_t> row_ptr;   // [states_size + 1]
   sqd::DevBuf<uint32_t> cols;     // [nnz] source index of each stored pair
   sqd::DevBuf<uint32_t> grps;     // [nnz] group index of each stored pair

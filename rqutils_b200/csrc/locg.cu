@@ -1099,8 +1099,7 @@ k_bmv_csr(const int64_t* __restrict__ row_ptr, const uint32_t* __restrict__ cols
       CAcc<R, NCV, NCA> acc;
       if (row < r1) {
         const int64_t b = __ldg(row_ptr + row), e = __ldg(row_ptr + row + 1);
-        for (int64_t i = b + sub; i < e; i += LPR)
-          acc.add(ld_elem<R, NCA>(vals, i), ld_elem<R, NCV>(v, __ldg(cols + i)));
+        csr_row_dot<R, NCV, NCA, LPR>(cols, vals, v, b + sub, e, acc);
       }
       acc.merge(LPR);
       if (sub == 0 && row < r1)

@@ -25,26 +25,34 @@ template <typename R, int NCV, int NCA, int LPR>
 __global__ void __launch_bounds__(256)
 k_mv_csr(const int64_t* __restrict__ row_ptr, const uint32_t* __restrict__ cols,
          const R* __restrict__ vals, const R* __restrict__ v, R* __restrict__ out,
-         int64_t n_rows) {
+         int64_t n_rows, int64_t chunk) {
   constexpr int RPW = 32 / LPR;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int sub = lane % LPR, slot = lane / LPR;
-  const int64_t w0 = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
-  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
-  for (int64_t rb = w0 * RPW; rb < n_rows; rb += nw * RPW) {
+  auto one_step = [&](int64_t rb, int64_t lim) {
     const int64_t row = rb + slot;
     CAcc<R, NCV, NCA> acc;
-    if (row < n_rows) {
+    if (row < lim) {
       const int64_t b = __ldg(row_ptr + row), e = __ldg(row_ptr + row + 1);
-      for (int64_t i = b + sub; i < e; i += LPR) {
-        const uint32_t c = __ldg(cols + i);
-        const Cx<R> a = ld_elem<R, NCA>(vals, i);
-        const Cx<R> x = ld_elem<R, NCV>(v, c);
-        acc.add(a, x);
-      }
+      csr_row_dot<R, NCV, NCA, LPR>(cols, vals, v, b + sub, e, acc);
     }
     acc.merge(LPR);
-    if (sub == 0 && row < n_rows) st_elem<R, NCV>(out, row, cx_make<R>(acc.re.value(), acc.im.value()));
+    if (sub == 0 && row < lim) st_elem<R, NCV>(out, row, cx_make<R>(acc.re.value(), acc.im.value()));
+  };
+  if (chunk <= 0) {
+    // Interleaved: consecutive warps of the grid take consecutive row groups.
+    const int64_t w0 = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+    const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t rb = w0 * RPW; rb < n_rows; rb += nw * RPW) one_step(rb, n_rows);
+  } else {
+    // Chunked: a block owns `chunk` consecutive rows at a time, so the source amplitudes its
+    // rows share (same high-sector block, neighbouring rows) are reused from its L1.
+    const int nwb = blockDim.x >> 5;
+    for (int64_t c0 = int64_t(blockIdx.x) * chunk; c0 < n_rows; c0 += int64_t(gridDim.x) * chunk) {
+      const int64_t lim = min(c0 + chunk, n_rows);
+      for (int64_t rb = c0 + int64_t(warp) * RPW; rb < lim; rb += int64_t(nwb) * RPW)
+        one_step(rb, lim);
+    }
   }
 }
 
@@ -178,8 +186,9 @@ void op_matvec(sqd_op_s* op, const void* v, void* out, int dtype, cudaStream_t s
           const R* vals;
           if constexpr (sizeof(R) == 8) vals = op->values.ptr;
           else vals = op->values32.ptr;
+          const int64_t chunk = op->chunk_rows[sizeof(R) == 8 ? 0 : 1];
           k_mv_csr<R, NCV, NCA, LPR><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, vals,
-                                                        vin, vout, size);
+                                                        vin, vout, size, chunk);
         } else {
           k_mv_xc<R, NCV, NCA, LPR><<<G, 256, 0, st>>>(
               op->row_ptr.ptr, op->cols.ptr, op->grps.ptr, sp->states.ptr, sp->n_unique,

@@ -487,6 +487,15 @@ extern "C" int sqd_op_set_lanes(sqd_op_t op, int precision, int lanes_per_row) {
   });
 }
 
+extern "C" int sqd_op_set_chunk(sqd_op_t op, int precision, int64_t chunk_rows) {
+  return guarded([&] {
+    SQD_REQUIRE(op != nullptr, "NULL operator");
+    SQD_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (FP32)");
+    SQD_REQUIRE(chunk_rows >= 0, "chunk_rows must be >= 0");
+    op->chunk_rows[precision] = chunk_rows;
+  });
+}
+
 extern "C" int sqd_op_get_lanes(sqd_op_t op, int precision, int* lanes_per_row) {
   return guarded([&] {
     SQD_REQUIRE(op != nullptr && lanes_per_row != nullptr, "NULL argument");

@@ -181,6 +181,15 @@ class SQDOperator:
         _lib.call('sqd_op_get_lanes', self._handle, int(precision), _lib._c.byref(v))
         return v.value
 
+    def set_chunk(self, precision, chunk_rows):
+        """Rows a thread block owns at a time in the cached matvec (0 = interleaved)."""
+        _lib.call('sqd_op_set_chunk', self._handle, int(precision), int(chunk_rows))
+        self._chunk = getattr(self, '_chunk', [0, 0])
+        self._chunk[precision] = int(chunk_rows)
+
+    def get_chunk(self, precision):
+        return getattr(self, '_chunk', [0, 0])[precision]
+
     def set_lanes(self, precision, lanes):
         """precision 0: FP64 vectors (float64/complex128), 1: FP32 vectors."""
         _lib.call('sqd_op_set_lanes', self._handle, int(precision), int(lanes))
