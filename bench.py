@@ -45,6 +45,7 @@ def parse():
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--cpu-rows', type=int, default=0, help='CPU sample rows (0 = auto)')
     ap.add_argument('--lanes', type=int, default=0, help='lanes per row (0 = autotune)')
+    ap.add_argument('--chunk', type=int, default=0, help='rows per block chunk with --lanes')
     return ap.parse_args()
 
 
@@ -267,7 +268,10 @@ def run_ours(args):
     setup_s = time.perf_counter() - t_setup0
     if args.lanes:
         op.lanes_per_row = args.lanes
-        tuned = {'lanes_per_row': args.lanes, 'note': 'fixed by --lanes'}
+        op.set_chunk(0, args.chunk)
+        op.set_chunk(1, args.chunk)
+        tuned = {'lanes_per_row': args.lanes, 'chunk_rows': args.chunk,
+                 'note': 'fixed by --lanes/--chunk'}
     else:
         tuned = op.autotune()
     n_rows = space.states_size
