@@ -8,7 +8,8 @@ A step is one Pauli-sum matvec Hv over the whole subspace (the inner kernel of L
 is row.terms/s = (rows x merged terms) / step time, summed over ranks (replicas, weak scaling),
 with inputs resident in HBM; ``e2e`` is the same metric through the public API with the input
 vector copied from pinned host memory and the result copied back inside the timed region.
-Beside it: the roofline of the matvec kernel, the LOCG time-to-E0 (FP64 and mixed precision),
+Beside it: the roofline of the matvec (its kernels together), the LOCG time-to-E0 (FP64 and
+mixed precision),
 and the CPU baseline (the reference's default matvec algorithm on the host cores, on a row
 sample).  ``--impl reference`` times only that CPU path.
 
@@ -46,6 +47,8 @@ def parse():
     ap.add_argument('--cpu-rows', type=int, default=0, help='CPU sample rows (0 = auto)')
     ap.add_argument('--lanes', type=int, default=0, help='lanes per row (0 = autotune)')
     ap.add_argument('--chunk', type=int, default=0, help='rows per block chunk with --lanes')
+    ap.add_argument('--layout', default='csr', choices=['csr', 'product'],
+                    help='element layout with --lanes (the autotuner picks it otherwise)')
     return ap.parse_args()
 
 
@@ -75,9 +78,10 @@ def load_peaks():
     return 6650.0, 'fallback'
 
 
-def load_traffic(workload, cache):
-    """DRAM traffic per launch of the matvec kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, 'profiles', f'matvec_{workload}_cache{cache[0]}{cache[1]}.md')
+def load_traffic(workload, cache, layout='csr'):
+    """DRAM traffic of one matvec (all its kernels) from the committed ncu summary."""
+    suffix = '' if layout == 'csr' else f'_{layout}'
+    path = os.path.join(ROOT, 'profiles', f'matvec_{workload}_cache{cache[0]}{cache[1]}{suffix}.md')
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -267,11 +271,12 @@ def run_ours(args):
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t_setup0
     if args.lanes:
+        for prec in (0, 1):
+            op.set_layout(prec, args.layout)
+            op.set_chunk(prec, args.chunk)
         op.lanes_per_row = args.lanes
-        op.set_chunk(0, args.chunk)
-        op.set_chunk(1, args.chunk)
-        tuned = {'lanes_per_row': args.lanes, 'chunk_rows': args.chunk,
-                 'note': 'fixed by --lanes/--chunk'}
+        tuned = {'layout': args.layout, 'lanes_per_row': args.lanes, 'chunk_rows': args.chunk,
+                 'note': 'fixed by --layout/--lanes/--chunk'}
     else:
         tuned = op.autotune()
     n_rows = space.states_size
@@ -300,7 +305,13 @@ def run_ours(args):
     t_local = ev0.elapsed_time(ev1) / 1e3
     units = n_rows * m_terms
     value, t_max = replica_throughput(units, args.steps, t_local, dist)
-    gpu_launches = args.steps
+    # kernels per matvec: CSR layout 1; product layout: transpose, low-half slabs, transpose,
+    # two-half CSR tails (when there are any), high-half slabs
+    layout = op.get_layout(0) if cache == (1, 2) else 'csr'
+    per_step = 1
+    if layout == 'product':
+        per_step = 5 if op.product_info()['pairs_mixed'] > 0 else 4
+    gpu_launches = args.steps * per_step
 
     # end to end: pinned host input -> device -> matvec -> pinned host output
     v_host = v.cpu().pin_memory()
@@ -329,7 +340,7 @@ def run_ours(args):
     bytes_alg = n_rows * (8 * W + 2 * w_v) + nnz * w_v + m_terms * (8 * W + w_c) + j_groups * 8 * W
     peak, peak_kind = load_peaks()
     achieved = bytes_alg / (t_local / args.steps) / 1e9
-    traffic = load_traffic(args.workload, cache)
+    traffic = load_traffic(args.workload, cache, layout)
 
     extra = {}
     if not args.no_locg and rank == 0:
@@ -346,6 +357,9 @@ def run_ours(args):
             'config': {**workload_config(wl, cache), 'parallelism': f'replicas x{world}',
                        'merged_terms': m_terms, 'x_groups': j_groups, 'stored_pairs': nnz,
                        'lanes_per_row': {'fp64': op.get_lanes(0), 'fp32': op.get_lanes(1)},
+                       'layout': {'fp64': layout,
+                                  'fp32': op.get_layout(1) if cache == (1, 2) else 'csr'},
+                       'kernels_per_matvec': per_step,
                        'autotune': tuned,
                        'setup_s': setup_s},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
@@ -353,7 +367,8 @@ def run_ours(args):
                          'peak_kind': peak_kind,
                          'bytes_alg_per_launch': bytes_alg,
                          'formula': 'N(8W+2w_v) + P_valid w_v + M(8W+w_c) + J 8W, W=1, '
-                                    'w_v=16, w_c=16, P_valid = stored pairs'},
+                                    'w_v=16, w_c=16, P_valid = stored pairs',
+                         'timed': 'one whole FP64 matvec (all its kernels) per launch'},
             'e2e': {'value': e2e_value, 'unit': UNIT,
                     'h2d_bytes_per_step': int(v.numel() * 16),
                     'd2h_bytes_per_step': int(v.numel() * 16)},

@@ -127,6 +127,23 @@ int sqd_op_get_lanes(sqd_op_t op, int precision, int* lanes_per_row);
  * > 0 = each thread block owns chunk_rows consecutive rows at a time (L1 reuse of the source
  * amplitudes that neighbouring rows share). */
 int sqd_op_set_chunk(sqd_op_t op, int precision, int64_t chunk_rows);
+/* Third knob of the cached matvec (no rqutils counterpart): the element layout it streams.
+ * SQD_LAYOUT_CSR: one (source, element) list per row.  SQD_LAYOUT_PRODUCT: for a subspace
+ * that is the product of strings on the high and the low half of the qubits (every high string
+ * with every low string, no fill-in slots), the pairs that change one half only are stored as
+ * dense slabs whose sources are implied by their position (coalesced loads, no index per
+ * pair); the pairs that change both halves keep their CSR lists (lanes and chunk knobs apply
+ * to those).  Setting SQD_LAYOUT_PRODUCT builds the slabs on first use (SQD_ERR_UNSUPPORTED
+ * when the subspace is not such a product); results equal the CSR layout's up to the order of
+ * each row's sum. */
+enum sqd_layout { SQD_LAYOUT_CSR = 0, SQD_LAYOUT_PRODUCT = 1 };
+int sqd_op_set_layout(sqd_op_t op, int precision, int layout, void* stream);
+int sqd_op_get_layout(sqd_op_t op, int precision, int* layout);
+/* Product structure: n_high x n_low rows (0, 0 when the subspace is not a product) and, once
+ * the slabs are built, the stored pairs in high-half slabs, low-half slabs and CSR tails (-1
+ * before). */
+int sqd_op_product_info(sqd_op_t op, void* stream, int64_t* n_high, int64_t* n_low,
+                        int64_t* pairs_high, int64_t* pairs_low, int64_t* pairs_mixed);
 /* Hv on the subspace (apply_h_x_cached and friends, sqd.py:643-743 via
  * make_x_cached_matvec sqd.py:746-751).  v and out have states_size elements of dtype. */
 int sqd_matvec(sqd_op_t op, const void* v, void* out, int dtype, void* stream);

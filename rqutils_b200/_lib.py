@@ -74,6 +74,10 @@ EXTRA_PROTOTYPES = {
     'sqd_batch_destroy': (None, [_vp]),
     'sqd_op_release_groups': (_i32, [_vp]),
     'sqd_op_set_chunk': (_i32, [_vp, _i32, _i64]),
+    'sqd_op_set_layout': (_i32, [_vp, _i32, _i32, _vp]),
+    'sqd_op_get_layout': (_i32, [_vp, _i32, _c.POINTER(_i32)]),
+    'sqd_op_product_info': (_i32, [_vp, _vp, _c.POINTER(_i64), _c.POINTER(_i64),
+                                   _c.POINTER(_i64), _c.POINTER(_i64), _c.POINTER(_i64)]),
 }
 
 

@@ -1,6 +1,9 @@
-// Matvec accumulators: plain FMA in FP64; in FP32 the compensated dot product of Ogita, Rump
-// and Oishi (SIAM J. Sci. Comput. 26, 2005): TwoProduct via fma and TwoSum, so the FP32 result is
-// as accurate as if accumulated in twice the working precision.
+// Matvec accumulators: plain FMA in FP64; in FP32 a compensated sum after Ogita, Rump and Oishi
+// (SIAM J. Sci. Comput. 26, 2005).  Single products (add) use their Dot2 step: TwoProduct via
+// fma and TwoSum, as accurate as twice the working precision.  The unrolled loops (add4) sum
+// four products by an FMA chain and compensate only the running sum: the elements are FP32
+// numbers already rounded once, so the chain's few roundings stay at that level, and the sum
+// over the row keeps a bounded error however long the row is.
 #pragma once
 #include "common.cuh"
 
@@ -23,6 +26,18 @@ struct Acc {
     }
   }
   __device__ __forceinline__ void add_neg_prod(R a, R b) { add_prod(-a, b); }
+  // s + p with the rounding error of the addition kept in c (TwoSum).
+  __device__ __forceinline__ void add_sum(R p) {
+    if constexpr (sizeof(R) == 8) {
+      s += p;
+    } else {
+      const R t = s + p;
+      const R bp = t - s;
+      const R es = (s - (t - bp)) + (p - bp);
+      s = t;
+      c += es;
+    }
+  }
   __device__ __forceinline__ void merge_lanes(int width) {
     for (int o = width >> 1; o > 0; o >>= 1) {
       const R os = __shfl_xor_sync(kFullMask, s, o);
@@ -39,6 +54,21 @@ struct Acc {
     }
   }
   __device__ __forceinline__ R value() const { return sizeof(R) == 8 ? s : s + c; }
+  // Partial sums kept in FP64 between kernels: the FP32 state (s, c) is exact in a double up
+  // to the double's rounding, and a double splits back into (hi, lo) floats.
+  __device__ __forceinline__ double value_d() const {
+    return sizeof(R) == 8 ? double(s) : double(s) + double(c);
+  }
+  __device__ __forceinline__ void add_d(double d) {
+    if constexpr (sizeof(R) == 8) {
+      s += d;
+    } else {
+      const R hi = static_cast<R>(d);
+      const R lo = static_cast<R>(d - double(hi));
+      add_sum(hi);
+      c += lo;
+    }
+  }
 };
 
 template <typename R, int NCV, int NCA>
@@ -52,9 +82,46 @@ struct CAcc {
       if constexpr (NCA == 2) im.add_prod(a.im, x.re);
     }
   }
+  // Four products at once.  FP64: four FMAs.  FP32: the products are summed by an FMA chain
+  // whose result enters the compensated sum.
+  __device__ __forceinline__ void add4(const Cx<R>* a, const Cx<R>* x) {
+    if constexpr (sizeof(R) == 8) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) add(a[u], x[u]);
+    } else {
+      R pr = 0, pi = 0;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        pr = fmaf(a[u].re, x[u].re, pr);
+        if constexpr (NCV == 2) {
+          if constexpr (NCA == 2) pr = fmaf(-a[u].im, x[u].im, pr);
+          pi = fmaf(a[u].re, x[u].im, pi);
+          if constexpr (NCA == 2) pi = fmaf(a[u].im, x[u].re, pi);
+        }
+      }
+      re.add_sum(pr);
+      if constexpr (NCV == 2) im.add_sum(pi);
+    }
+  }
   __device__ __forceinline__ void merge(int width) {
     re.merge_lanes(width);
     if constexpr (NCV == 2) im.merge_lanes(width);
+  }
+  // FP64 partial at element i of a double array (NCV doubles per element).
+  __device__ __forceinline__ void add_partial(const double* p, int64_t i) {
+    if constexpr (NCV == 2) {
+      const double2 d = reinterpret_cast<const double2*>(p)[i];
+      re.add_d(d.x);
+      im.add_d(d.y);
+    } else {
+      re.add_d(p[i]);
+    }
+  }
+  __device__ __forceinline__ void store_partial(double* p, int64_t i) const {
+    if constexpr (NCV == 2)
+      reinterpret_cast<double2*>(p)[i] = make_double2(re.value_d(), im.value_d());
+    else
+      p[i] = re.value_d();
   }
 };
 
@@ -76,8 +143,7 @@ __device__ __forceinline__ void csr_row_dot(const uint32_t* __restrict__ cols,
       a[u] = ld_elem<R, NCA>(vals, i + u * LPR);
       x[u] = ld_elem<R, NCV>(v, c[u]);
     }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) acc.add(a[u], x[u]);
+    acc.add4(a, x);
   }
   for (; i < e; i += LPR) acc.add(ld_elem<R, NCA>(vals, i), ld_elem<R, NCV>(v, __ldg(cols + i)));
 }

@@ -50,11 +50,38 @@ struct sqd_space_s {
 
 constexpr int kBitmapLog2 = 17;
 
+namespace sqd {
+// Low half of the qubits (bits 0 .. n/2 - 1): the low sector of the conserved-weight sectors and
+// of the product layout.
+inline uint64_t half_mask_low(int num_qubits) {
+  const int h = num_qubits / 2;
+  return h == 0 ? 0ull : ((1ull << h) - 1ull);
+}
+}  // namespace sqd
+
 // Per-group data for the connectivity sweep.
 struct GroupPre {
   uint64_t x;
   int32_t group;     // group index j
   int32_t cx;        // popcount(x & sector_mask[l]) packed as bytes (l = 0, 1)
+};
+
+// Product-subspace layout of the cached matvec (product.cu).  Rows r = h * nl + l.  H entries
+// of slab h: k in [ho[h], ho[h+1]), source offset hsrc[k] = h' * nl, elements vh at
+// panel-major ((l / 32) * th + k) * 32 + l % 32; L entries of low string l: e in
+// [lo[l], lo[l+1]), source offset lsrc[e] = l' * nh (into the transposed vector), elements vl
+// at ((h / 32) * tl + e) * 32 + h % 32.  The rest of a row (M pairs) stays in the CSR arrays
+// after the first (ho[h+1] - ho[h]) + (lo[l+1] - lo[l]) pairs.
+struct ProductLayout {
+  int built = 0;
+  int64_t nh = 0, nl = 0;
+  int64_t th = 0, tl = 0;            // H and L entries over all slabs
+  int64_t pairs_h = 0, pairs_l = 0, pairs_m = 0;
+  sqd::DevBuf<int64_t> ho, lo;       // [nh + 1], [nl + 1]
+  sqd::DevBuf<uint32_t> hsrc, lsrc;  // [th], [tl]
+  sqd::DevBuf<double> vh, vl;        // FP64 elements (x2 interleaved when complex)
+  sqd::DevBuf<float> vh32, vl32;     // FP32 copies
+  sqd::DevBuf<double> vt, tt, t;     // per-matvec scratch: transposed input, L and M partials
 };
 
 struct sqd_op_s {
@@ -74,6 +101,8 @@ struct sqd_op_s {
   sqd::DevBuf<GroupPre> gpre;     // groups that can connect (x != 0, even sector counts)
   int64_t n_gpre = 0;
   sqd::DevBuf<int> status;        // device status word
+  int layout[2] = {0, 0};         // SQD_LAYOUT_* per precision
+  ProductLayout prod;
 };
 
 namespace sqd {
@@ -111,5 +140,11 @@ __device__ __forceinline__ uint32_t sector_bitmap_index(uint64_t proj, int shift
 void op_build(sqd_op_s* op, cudaStream_t st);
 void op_matvec(sqd_op_s* op, const void* v, void* out, int dtype, cudaStream_t st);
 void op_ensure_values32(sqd_op_s* op, cudaStream_t st);
+// Product layout (product.cu).
+bool op_product_detect(sqd_op_s* op, cudaStream_t st, int64_t* nh, int64_t* nl);
+void op_product_build(sqd_op_s* op, cudaStream_t st);
+void op_product_values(sqd_op_s* op, cudaStream_t st);
+void op_product_values32(sqd_op_s* op, cudaStream_t st);
+void op_product_matvec(sqd_op_s* op, const void* v, void* out, int dtype, cudaStream_t st);
 
 }  // namespace sqd

@@ -172,6 +172,11 @@ void op_matvec(sqd_op_s* op, const void* v, void* out, int dtype, cudaStream_t s
   sqd_space_s* sp = op->s;
   const int64_t size = sp->states_size;
   if (op->x_cache == 1 && op->z_cache == 2 && !dtype_is_double(dtype)) op_ensure_values32(op, st);
+  if (op->x_cache == 1 && op->z_cache == 2 && op->prod.built &&
+      op->layout[dtype_is_double(dtype) ? 0 : 1] != SQD_LAYOUT_CSR) {
+    op_product_matvec(op, v, out, dtype, st);
+    return;
+  }
   dispatch_vec(dtype, op->value_complex, [&](auto rt, auto ncv_t, auto nca_t) {
     using R = typename decltype(rt)::type;
     constexpr int NCV = decltype(ncv_t)::value;

@@ -14,37 +14,44 @@
 namespace sqd {
 namespace {
 
-// Groups that can connect, split in two classes so that the class-0 groups come first in every
-// row's stored pairs.  Class 0 (two sectors only): groups acting on the high sector alone.  In
-// an alpha x beta product subspace all rows with the same beta string have the same class-0
-// connections, so a warp serving consecutive rows gathers adjacent amplitudes for them.
+// Groups that can connect, in three classes so that every row's stored pairs come in class
+// order.  With the qubits split in a low half (mask mlo) and a high half (mhi):
+//   class 0 (H): x acts on the high half only;
+//   class 1 (L): x acts on the low half only;
+//   class 2 (M): x acts on both halves.
+// In an alpha x beta product subspace all rows with the same high string have the same class-0
+// sources and all rows with the same low string the same class-1 sources, which the product
+// layout of the matvec (product.cu) builds on.  Inside a class the group order is kept.
 __global__ void k_gpre_flags(const uint64_t* group_x, int64_t J, int nsec, uint64_t m0,
-                             uint64_t m1, int64_t* flags0, int64_t* flags1) {
+                             uint64_t m1, uint64_t mlo, uint64_t mhi, int64_t* flags0,
+                             int64_t* flags1, int64_t* flags2) {
   for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < J;
        j += int64_t(gridDim.x) * blockDim.x) {
     const uint64_t x = group_x[j];
     bool ok = x != 0;
     if (nsec > 0) ok = ok && ((__popcll(x & m0) & 1) == 0);
     if (nsec > 1) ok = ok && ((__popcll(x & m1) & 1) == 0);
-    const bool first = nsec > 1 && (x & m0) == 0;
-    flags0[j] = (ok && first) ? 1 : 0;
-    flags1[j] = (ok && !first) ? 1 : 0;
+    const int cls = (x & mlo) == 0 ? 0 : (x & mhi) == 0 ? 1 : 2;
+    flags0[j] = (ok && cls == 0) ? 1 : 0;
+    flags1[j] = (ok && cls == 1) ? 1 : 0;
+    flags2[j] = (ok && cls == 2) ? 1 : 0;
   }
 }
 
 __global__ void k_gpre_fill(const uint64_t* group_x, int64_t J, const int64_t* flags0,
                             const int64_t* pos0, const int64_t* flags1, const int64_t* pos1,
-                            uint64_t m0, uint64_t m1, GroupPre* out) {
-  const int64_t n0 = pos0[J];
+                            const int64_t* flags2, const int64_t* pos2, uint64_t m0, uint64_t m1,
+                            GroupPre* out) {
+  const int64_t n0 = pos0[J], n1 = pos1[J];
   for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < J;
        j += int64_t(gridDim.x) * blockDim.x) {
-    if (!flags0[j] && !flags1[j]) continue;
+    if (!flags0[j] && !flags1[j] && !flags2[j]) continue;
     const uint64_t x = group_x[j];
     GroupPre g;
     g.x = x;
     g.group = static_cast<int32_t>(j);
     g.cx = (__popcll(x & m0) & 0xff) | ((__popcll(x & m1) & 0xff) << 8);
-    out[flags0[j] ? pos0[j] : n0 + pos1[j]] = g;
+    out[flags0[j] ? pos0[j] : flags1[j] ? n0 + pos1[j] : n0 + n1 + pos2[j]] = g;
   }
 }
 
@@ -332,24 +339,27 @@ void op_build(sqd_op_s* op, cudaStream_t st) {
 
   // Groups that can connect.
   {
-    DevBuf<int64_t> flags0, pos0, flags1, pos1;
-    flags0.alloc(J, st);
-    pos0.alloc(J + 1, st);
-    flags1.alloc(J, st);
-    pos1.alloc(J + 1, st);
+    DevBuf<int64_t> flags[3], pos[3];
+    for (int c = 0; c < 3; ++c) {
+      flags[c].alloc(J, st);
+      pos[c].alloc(J + 1, st);
+    }
+    const uint64_t mlo = half_mask_low(sp->num_qubits), mhi = sp->fill_state & ~mlo;
     const unsigned G = grid_for(J, 256, 4096);
     k_gpre_flags<<<G, 256, 0, st>>>(p->group_x.ptr, J, sp->num_sectors, sp->sector_mask[0],
-                                   sp->sector_mask[1], flags0.ptr, flags1.ptr);
+                                   sp->sector_mask[1], mlo, mhi, flags[0].ptr, flags[1].ptr,
+                                   flags[2].ptr);
     SQD_CHECK_LAUNCH();
-    exclusive_scan_i64(flags0.ptr, pos0.ptr, J, true, st);
-    exclusive_scan_i64(flags1.ptr, pos1.ptr, J, true, st);
-    int64_t n0 = 0, n1 = 0;
-    copy_to_host(&n0, pos0.ptr + J, 1, st);
-    copy_to_host(&n1, pos1.ptr + J, 1, st);
-    op->n_gpre = n0 + n1;
+    int64_t n_cls[3] = {0, 0, 0};
+    for (int c = 0; c < 3; ++c) {
+      exclusive_scan_i64(flags[c].ptr, pos[c].ptr, J, true, st);
+      copy_to_host(&n_cls[c], pos[c].ptr + J, 1, st);
+    }
+    op->n_gpre = n_cls[0] + n_cls[1] + n_cls[2];
     op->gpre.alloc(op->n_gpre > 0 ? op->n_gpre : 1, st);
-    k_gpre_fill<<<G, 256, 0, st>>>(p->group_x.ptr, J, flags0.ptr, pos0.ptr, flags1.ptr, pos1.ptr,
-                                  sp->sector_mask[0], sp->sector_mask[1], op->gpre.ptr);
+    k_gpre_fill<<<G, 256, 0, st>>>(p->group_x.ptr, J, flags[0].ptr, pos[0].ptr, flags[1].ptr,
+                                  pos[1].ptr, flags[2].ptr, pos[2].ptr, sp->sector_mask[0],
+                                  sp->sector_mask[1], op->gpre.ptr);
     SQD_CHECK_LAUNCH();
   }
   if (op->x_cache == 0) return;
@@ -436,11 +446,14 @@ void op_build(sqd_op_s* op, cudaStream_t st) {
 }
 
 void op_ensure_values32(sqd_op_s* op, cudaStream_t st) {
-  if (op->values32.ptr || op->z_cache != 2 || op->nnz == 0) return;
-  const size_t n = static_cast<size_t>(op->nnz) * (op->value_complex ? 2 : 1);
-  op->values32.alloc(n, st);
-  k_to_float<<<grid_for(n, 256, 16384), 256, 0, st>>>(op->values.ptr, op->values32.ptr, n);
-  SQD_CHECK_LAUNCH();
+  if (op->z_cache != 2 || op->nnz == 0) return;
+  if (!op->values32.ptr) {
+    const size_t n = static_cast<size_t>(op->nnz) * (op->value_complex ? 2 : 1);
+    op->values32.alloc(n, st);
+    k_to_float<<<grid_for(n, 256, 16384), 256, 0, st>>>(op->values.ptr, op->values32.ptr, n);
+    SQD_CHECK_LAUNCH();
+  }
+  op_product_values32(op, st);
 }
 
 }  // namespace sqd
@@ -628,6 +641,7 @@ extern "C" int sqd_op_refresh(sqd_op_t op, void* stream) {
       k_to_float<<<grid_for(n, 256, 16384), 256, 0, st>>>(op->values.ptr, op->values32.ptr, n);
       SQD_CHECK_LAUNCH();
     }
+    op_product_values(op, st);
   });
 }
 

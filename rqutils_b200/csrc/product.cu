@@ -1,0 +1,591 @@
+// Product-subspace layout of the cached matvec (cache_strategy (1, 2)).
+//
+// SQD subspaces are usually the Cartesian product of strings on the high half of the qubits
+// (beta) and strings on the low half (alpha).  Sorted, row r = h * nl + l holds H[h] | L[l].
+// The stored pairs of a row come in three classes (k_gpre_flags, operator.cu):
+//   H: x on the high half only, source (h', l) with H[h'] = H[h] ^ x.  Every row of slab h has
+//      the same H sources in the same order;
+//   L: the diagonal group and x on the low half only, source (h, l') with L[l'] = L[l] ^ x.
+//      Every row with low string l has the same L sources in the same order;
+//   M: the rest (both halves change).
+// An H or L source is implied by (slab, position), so the elements of those pairs are laid out
+// again as dense slabs and the matvec streams them with coalesced loads and gathers v (or its
+// transpose vT[l][h]) with coalesced loads too, instead of one scattered gather and one index
+// per pair.  One matvec is six launches:
+//   1. vT = transpose(v)                                (32 x 32 tiles through shared memory)
+//   2. t2[l][h] = sum_e VL(lo[l] + e, h) vT[l'_e][h]     (L part; FP64 partial)
+//   3. t2' = transpose(t2) into the vT buffer           (now [h][l])
+//   4. t3[r] = sum of the row's M pairs                  (CSR, LPR lanes per row; FP64 partial)
+//   5. out[h][l] = t2'[h][l] + t3[r] + sum_k VH(ho[h] + k, l) v[h'_k][l]
+// Steps 2 and 5 are one kernel (k_slab) over an A x B grid of outputs (A slabs of B rows each,
+// A = nh for H, A = nl for L): a warp owns one slab a and 32 consecutive b (one "panel"), a
+// block 8 slabs of the same panel, and blocks run panel-major, so the 32-wide panel of the
+// gathered vector stays in L2 while all slabs pass over it.  The elements are stored in the
+// same panel-major order, VH(k, l) at ((l / 32) * KH + k) * 32 + l % 32 (KH = entries of all
+// slabs), so the element stream of a panel pass is one contiguous sweep.  Source indices are
+// kept premultiplied (h' * nl, l' * nh).  Both slab passes are bound by the L2 -> SM traffic of
+// the coalesced amplitude reads (one amplitude per entry, served by L2) rather than by DRAM.
+// FP32 vectors keep the compensated accumulation in every part and pass partials in FP64, so
+// the result is rounded once.  The elements are the same numbers as in the CSR arrays; only
+// the summation order of a row changes (L and M pairs before H pairs).
+#include <algorithm>
+#include <climits>
+#include <type_traits>
+
+#include "internal.cuh"
+#include "dispatch.cuh"
+#include "accum.cuh"
+
+namespace sqd {
+namespace {
+
+__device__ __forceinline__ void warp_count_add(unsigned long long c, unsigned long long* dst) {
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFullMask, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(dst, c);
+}
+
+// Number of distinct high strings (rows whose high half differs from the previous row's).
+__global__ void k_count_slabs(const uint64_t* __restrict__ s, int64_t n, uint64_t mhi,
+                              unsigned long long* cnt) {
+  unsigned long long c = 0;
+  for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n;
+       r += int64_t(gridDim.x) * blockDim.x)
+    if (r == 0 || ((s[r] ^ s[r - 1]) & mhi) != 0) ++c;
+  warp_count_add(c, cnt);
+}
+
+// Rows that are not H[r / nl] | L[r % nl].
+__global__ void k_check_product(const uint64_t* __restrict__ s, int64_t n, int64_t nl,
+                                uint64_t mlo, uint64_t mhi, unsigned long long* bad) {
+  unsigned long long c = 0;
+  for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n;
+       r += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t l = r % nl;
+    const uint64_t v = s[r];
+    if (((v ^ s[l]) & mlo) != 0 || ((v ^ s[r - l]) & mhi) != 0) ++c;
+  }
+  warp_count_add(c, bad);
+}
+
+// Per row: the H pairs that follow the diagonal entry and the L pairs after them; a pair of
+// another class before the M pairs end counts as an error.
+__global__ void k_row_kinds(const int64_t* __restrict__ row_ptr, const uint32_t* __restrict__ grps,
+                            const uint64_t* __restrict__ group_x, int64_t n, int d, uint64_t mlo,
+                            uint64_t mhi, int32_t* rkh, int32_t* rkl, unsigned long long* bad) {
+  unsigned long long c = 0;
+  for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n;
+       r += int64_t(gridDim.x) * blockDim.x) {
+    int64_t i = row_ptr[r];
+    const int64_t e = row_ptr[r + 1];
+    bool ok = true;
+    if (d) {
+      ok = i < e && grps[i] == 0;
+      ++i;
+    }
+    const int64_t b = i;
+    while (i < e && (__ldg(group_x + grps[i]) & mlo) == 0) ++i;
+    const int64_t b2 = i;
+    while (i < e && (__ldg(group_x + grps[i]) & mhi) == 0) ++i;
+    const int64_t b3 = i;
+    for (; i < e; ++i) {
+      const uint64_t x = __ldg(group_x + grps[i]);
+      if ((x & mlo) == 0 || (x & mhi) == 0) ok = false;
+    }
+    rkh[r] = static_cast<int32_t>(b2 - b);
+    rkl[r] = static_cast<int32_t>(b3 - b2);
+    if (!ok) ++c;
+  }
+  warp_count_add(c, bad);
+}
+
+// Entries per slab (from the slab's first row) and per low string (from slab 0, diagonal
+// included); every row must agree with both.
+__global__ void k_slab_meta(const int32_t* __restrict__ rkh, const int32_t* __restrict__ rkl,
+                            int64_t n, int64_t nl, int d, int64_t* kh, int64_t* kl,
+                            unsigned long long* bad) {
+  unsigned long long c = 0;
+  for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n;
+       r += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t h = r / nl, l = r - h * nl;
+    if (l == 0) kh[h] = rkh[r];
+    if (h == 0) kl[l] = d + rkl[r];
+    if (rkh[r] != rkh[h * nl] || rkl[r] != rkl[l]) ++c;
+  }
+  warp_count_add(c, bad);
+}
+
+// H sources as offsets h' * nl: the sources of row (h, 0) itself.
+__global__ void k_hsrc(const int64_t* __restrict__ row_ptr, const uint32_t* __restrict__ cols,
+                       int64_t nh, int64_t nl, int d, const int64_t* __restrict__ ho,
+                       uint32_t* hsrc) {
+  for (int64_t h = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; h < nh;
+       h += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t b = row_ptr[h * nl] + d;
+    for (int64_t k = 0; k < ho[h + 1] - ho[h]; ++k) hsrc[ho[h] + k] = cols[b + k];
+  }
+}
+
+// L sources as offsets l' * nh (into the transposed vector), from row (0, l).
+__global__ void k_lsrc(const int64_t* __restrict__ row_ptr, const uint32_t* __restrict__ cols,
+                       int64_t nh, int64_t nl, int d, const int64_t* __restrict__ ho,
+                       const int64_t* __restrict__ lo, uint32_t* lsrc) {
+  const int64_t kh0 = ho[1] - ho[0];
+  for (int64_t l = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; l < nl;
+       l += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t b = row_ptr[l];
+    for (int64_t e = 0; e < lo[l + 1] - lo[l]; ++e) {
+      const int64_t lp = (d && e == 0) ? l : int64_t(cols[b + kh0 + e]);
+      lsrc[lo[l] + e] = static_cast<uint32_t>(lp * nh);
+    }
+  }
+}
+
+// Panel-major slab index of entry k at contiguous position b.
+__device__ __forceinline__ int64_t panel_index(int64_t k, int64_t b, int64_t total_k) {
+  return ((b >> 5) * total_k + k) * 32 + (b & 31);
+}
+
+// Copies every H and L element into its slab and checks that its stored source is the one the
+// slab position implies.
+template <int NCA>
+__global__ void k_prod_extract(const int64_t* __restrict__ row_ptr,
+                               const uint32_t* __restrict__ cols, const double* __restrict__ vals,
+                               int64_t n, int64_t nh, int64_t nl, int d,
+                               const int64_t* __restrict__ ho, const int64_t* __restrict__ lo,
+                               const uint32_t* __restrict__ hsrc,
+                               const uint32_t* __restrict__ lsrc, double* vh, double* vl,
+                               int check, unsigned long long* bad) {
+  const int64_t th = ho[nh], tl = lo[nl];
+  unsigned long long c = 0;
+  for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n;
+       r += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t h = r / nl, l = r - h * nl;
+    const int64_t b = row_ptr[r];
+    const int64_t h0 = ho[h], nkh = ho[h + 1] - h0, l0 = lo[l], nkl = lo[l + 1] - l0;
+    if (check && row_ptr[r + 1] < b + nkh + nkl) {
+      ++c;
+      continue;
+    }
+    for (int64_t k = 0; k < nkh; ++k) {
+      const int64_t p = b + d + k;
+      if (check && int64_t(cols[p]) != int64_t(hsrc[h0 + k]) + l) ++c;
+      const int64_t q = panel_index(h0 + k, l, th);
+#pragma unroll
+      for (int t = 0; t < NCA; ++t) vh[NCA * q + t] = vals[NCA * p + t];
+    }
+    for (int64_t e = 0; e < nkl; ++e) {
+      const int64_t p = (d && e == 0) ? b : b + nkh + e;
+      if (check && int64_t(cols[p]) != h * nl + int64_t(lsrc[l0 + e]) / nh) ++c;
+      const int64_t q = panel_index(l0 + e, h, tl);
+#pragma unroll
+      for (int t = 0; t < NCA; ++t) vl[NCA * q + t] = vals[NCA * p + t];
+    }
+  }
+  warp_count_add(c, bad);
+}
+
+__global__ void k_to_float32(const double* __restrict__ in, float* __restrict__ out, int64_t n) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = static_cast<float>(in[i]);
+}
+
+// out[c][r] = in[r][c] for an rows x cols matrix of elements E (32 x 32 tiles, 256 threads).
+template <typename E>
+__global__ void __launch_bounds__(256)
+k_transpose(const E* __restrict__ in, E* __restrict__ out, int64_t rows, int64_t cols) {
+  __shared__ E tile[32][33];
+  const int64_t tr = (rows + 31) / 32, tc = (cols + 31) / 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int64_t t = blockIdx.x; t < tr * tc; t += gridDim.x) {
+    const int64_t r0 = (t / tc) * 32, c0 = (t % tc) * 32;
+    for (int i = ty; i < 32; i += 8) {
+      const int64_t r = r0 + i, c = c0 + tx;
+      if (r < rows && c < cols) tile[i][tx] = in[r * cols + c];
+    }
+    __syncthreads();
+    for (int i = ty; i < 32; i += 8) {
+      const int64_t c = c0 + i, r = r0 + tx;
+      if (c < cols && r < rows) out[c * rows + r] = tile[tx][i];
+    }
+    __syncthreads();
+  }
+}
+
+// One slab pass over an A x B grid: element (a, b) accumulates VS(k, b) * x[src[k] + b] over
+// k in [off[a], off[a + 1]) (VS panel-major over total_k entries, src premultiplied).  Warp =
+// one slab a and a 32-wide panel of b; block = 8 slabs of one panel; blocks panel-major.
+//   FINAL = false: store the FP64 partial at out_part[a * B + b];
+//   FINAL = true:  start from part_t[a * B + b] (+ part_m[a * B + b] when HAS_M) and store the
+//                  result at out[a * B + b].
+// Eight entries per step keep eight independent index -> amplitude chains in flight.
+template <typename R, int NCV, int NCA, bool FINAL, bool HAS_M>
+__global__ void __launch_bounds__(256)
+k_slab(int64_t A, int64_t B, int64_t total_k, int64_t a_tiles, const int64_t* __restrict__ off,
+       const uint32_t* __restrict__ src, const R* __restrict__ V, const R* __restrict__ x,
+       const double* __restrict__ part_t, const double* __restrict__ part_m, R* __restrict__ out,
+       double* __restrict__ out_part) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t panels = (B + 31) >> 5;
+  for (int64_t blk = blockIdx.x; blk < panels * a_tiles; blk += gridDim.x) {
+    const int64_t p = blk / a_tiles;
+    const int64_t a = (blk - p * a_tiles) * 8 + warp;
+    const int64_t b = p * 32 + lane;
+    if (a >= A || b >= B) continue;
+    CAcc<R, NCV, NCA> acc;
+    if constexpr (FINAL) {
+      acc.add_partial(part_t, a * B + b);
+      if constexpr (HAS_M) acc.add_partial(part_m, a * B + b);
+    }
+    const int64_t k1 = __ldg(off + a + 1);
+    int64_t k = __ldg(off + a);
+    const R* vp = V + ((p * total_k + k) * 32 + lane) * NCA;
+    for (; k + 7 < k1; k += 8) {
+      uint32_t si[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) si[u] = __ldg(src + k + u);
+      Cx<R> m[8], xv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        m[u] = ld_elem<R, NCA>(vp, 32 * u);
+        xv[u] = ld_elem<R, NCV>(x, int64_t(si[u]) + b);
+      }
+      acc.add4(m, xv);
+      acc.add4(m + 4, xv + 4);
+      vp += 8 * 32 * NCA;
+    }
+    for (; k < k1; ++k) {
+      acc.add(ld_elem<R, NCA>(vp, 0), ld_elem<R, NCV>(x, int64_t(__ldg(src + k)) + b));
+      vp += 32 * NCA;
+    }
+    if constexpr (FINAL) st_elem<R, NCV>(out, a * B + b, cx_make<R>(acc.re.value(), acc.im.value()));
+    else acc.store_partial(out_part, a * B + b);
+  }
+}
+
+// M pairs of every row (the CSR tail after the row's H and L entries), FP64 partial per row.
+// Same schedule as the CSR matvec: LPR lanes per row, interleaved or chunked rows.
+template <typename R, int NCV, int NCA, int LPR>
+__global__ void __launch_bounds__(256)
+k_mv_mixed(const int64_t* __restrict__ row_ptr, const uint32_t* __restrict__ cols,
+           const R* __restrict__ vals, const R* __restrict__ v, const int64_t* __restrict__ ho,
+           const int64_t* __restrict__ lo, int64_t nl, double* __restrict__ part,
+           int64_t n_rows, int64_t chunk) {
+  constexpr int RPW = 32 / LPR;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sub = lane % LPR, slot = lane / LPR;
+  auto one_step = [&](int64_t rb, int64_t lim) {
+    const int64_t row = rb + slot;
+    CAcc<R, NCV, NCA> acc;
+    if (row < lim) {
+      const int64_t h = row / nl, l = row - h * nl;
+      const int64_t skip =
+          (__ldg(ho + h + 1) - __ldg(ho + h)) + (__ldg(lo + l + 1) - __ldg(lo + l));
+      const int64_t b = __ldg(row_ptr + row) + skip, e = __ldg(row_ptr + row + 1);
+      csr_row_dot<R, NCV, NCA, LPR>(cols, vals, v, b + sub, e, acc);
+    }
+    acc.merge(LPR);
+    if (sub == 0 && row < lim) acc.store_partial(part, row);
+  };
+  if (chunk <= 0) {
+    const int64_t w0 = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+    const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t rb = w0 * RPW; rb < n_rows; rb += nw * RPW) one_step(rb, n_rows);
+  } else {
+    const int nwb = blockDim.x >> 5;
+    for (int64_t c0 = int64_t(blockIdx.x) * chunk; c0 < n_rows; c0 += int64_t(gridDim.x) * chunk) {
+      const int64_t lim = min(c0 + chunk, n_rows);
+      for (int64_t rb = c0 + int64_t(warp) * RPW; rb < lim; rb += int64_t(nwb) * RPW)
+        one_step(rb, lim);
+    }
+  }
+}
+
+unsigned capped_grid(int64_t blocks) {
+  return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(blocks, INT_MAX)));
+}
+
+template <typename R, int NCV, int NCA, bool FINAL, bool HAS_M>
+void launch_slab(int64_t A, int64_t B, int64_t total_k, const int64_t* off, const uint32_t* src,
+                 const R* V, const R* x, const double* part_t, const double* part_m, R* out,
+                 double* out_part, cudaStream_t st) {
+  if (A == 0 || B == 0) return;
+  const int64_t a_tiles = (A + 7) / 8, panels = (B + 31) / 32;
+  k_slab<R, NCV, NCA, FINAL, HAS_M><<<capped_grid(a_tiles * panels), 256, 0, st>>>(
+      A, B, total_k, a_tiles, off, src, V, x, part_t, part_m, out, out_part);
+  SQD_CHECK_LAUNCH();
+}
+
+template <typename E>
+void launch_transpose(const void* in, void* out, int64_t rows, int64_t cols, cudaStream_t st) {
+  const unsigned G = capped_grid(
+      std::min<int64_t>(((rows + 31) / 32) * ((cols + 31) / 32), int64_t(num_sms()) * 32));
+  k_transpose<E><<<G, 256, 0, st>>>(static_cast<const E*>(in), static_cast<E*>(out), rows, cols);
+  SQD_CHECK_LAUNCH();
+}
+
+unsigned mixed_grid(int64_t rows, int lpr) {
+  const int64_t warps = (rows * lpr + 31) / 32;
+  const int64_t blocks = (warps + 7) / 8;
+  const int64_t cap = static_cast<int64_t>(num_sms()) * 16;
+  return static_cast<unsigned>(std::max<int64_t>(1, std::min(blocks, cap)));
+}
+
+void extract(sqd_op_s* op, cudaStream_t st, int check, unsigned long long* bad) {
+  ProductLayout& L = op->prod;
+  const int64_t n = L.nh * L.nl;
+  const unsigned G = grid_for(n, 256, 16384);
+  if (op->value_complex)
+    k_prod_extract<2><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, op->values.ptr, n, L.nh,
+                                         L.nl, op->has_diag_group, L.ho.ptr, L.lo.ptr,
+                                         L.hsrc.ptr, L.lsrc.ptr, L.vh.ptr, L.vl.ptr, check, bad);
+  else
+    k_prod_extract<1><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, op->values.ptr, n, L.nh,
+                                         L.nl, op->has_diag_group, L.ho.ptr, L.lo.ptr,
+                                         L.hsrc.ptr, L.lsrc.ptr, L.vh.ptr, L.vl.ptr, check, bad);
+  SQD_CHECK_LAUNCH();
+}
+
+void to_float(const DevBuf<double>& in, DevBuf<float>& out, cudaStream_t st) {
+  out.alloc(in.count, st);
+  k_to_float32<<<grid_for(static_cast<int64_t>(in.count), 256, 16384), 256, 0, st>>>(
+      in.ptr, out.ptr, static_cast<int64_t>(in.count));
+  SQD_CHECK_LAUNCH();
+}
+
+}  // namespace
+
+bool op_product_detect(sqd_op_s* op, cudaStream_t st, int64_t* nh_out, int64_t* nl_out) {
+  sqd_space_s* sp = op->s;
+  const int64_t n = sp->n_unique;
+  *nh_out = *nl_out = 0;
+  if (n == 0 || sp->states_size != n || sp->num_qubits < 2) return false;
+  const uint64_t mlo = half_mask_low(sp->num_qubits), mhi = sp->fill_state & ~mlo;
+  DevBuf<unsigned long long> cnt;
+  cnt.alloc(2, st);
+  SQD_CUDA(cudaMemsetAsync(cnt.ptr, 0, 2 * sizeof(unsigned long long), st));
+  const unsigned G = grid_for(n, 256, 4096);
+  k_count_slabs<<<G, 256, 0, st>>>(sp->states.ptr, n, mhi, cnt.ptr);
+  SQD_CHECK_LAUNCH();
+  unsigned long long nh = 0;
+  copy_to_host(&nh, cnt.ptr, 1, st);
+  if (nh == 0 || n % static_cast<int64_t>(nh) != 0) return false;
+  const int64_t nl = n / static_cast<int64_t>(nh);
+  k_check_product<<<G, 256, 0, st>>>(sp->states.ptr, n, nl, mlo, mhi, cnt.ptr + 1);
+  SQD_CHECK_LAUNCH();
+  unsigned long long bad = 0;
+  copy_to_host(&bad, cnt.ptr + 1, 1, st);
+  if (bad) return false;
+  *nh_out = static_cast<int64_t>(nh);
+  *nl_out = nl;
+  return true;
+}
+
+void op_product_build(sqd_op_s* op, cudaStream_t st) {
+  if (op->prod.built) return;
+  SQD_REQUIRE(op->x_cache == 1 && op->z_cache == 2,
+              "the product layout needs cache_strategy (1, 2)");
+  SQD_REQUIRE(op->nnz == 0 || op->grps.ptr != nullptr,
+              "the operator released its group indices; create a new operator");
+  int64_t nh = 0, nl = 0;
+  if (!op_product_detect(op, st, &nh, &nl))
+    throw Error(SQD_ERR_UNSUPPORTED,
+                "the subspace is not a product of high-half and low-half strings without "
+                "fill-in slots; the product layout does not apply");
+  sqd_space_s* sp = op->s;
+  const uint64_t mlo = half_mask_low(sp->num_qubits), mhi = sp->fill_state & ~mlo;
+  const int d = op->has_diag_group;
+  const int64_t n = nh * nl;
+  ProductLayout L;
+  L.nh = nh;
+  L.nl = nl;
+  DevBuf<unsigned long long> bad;
+  bad.alloc(1, st);
+  SQD_CUDA(cudaMemsetAsync(bad.ptr, 0, sizeof(unsigned long long), st));
+  {
+    DevBuf<int32_t> rkh, rkl;
+    rkh.alloc(n, st);
+    rkl.alloc(n, st);
+    DevBuf<int64_t> kh, kl;
+    kh.alloc(nh, st);
+    kl.alloc(nl, st);
+    const unsigned G = grid_for(n, 256, 16384);
+    k_row_kinds<<<G, 256, 0, st>>>(op->row_ptr.ptr, op->grps.ptr, op->p->group_x.ptr, n, d, mlo,
+                                   mhi, rkh.ptr, rkl.ptr, bad.ptr);
+    SQD_CHECK_LAUNCH();
+    k_slab_meta<<<G, 256, 0, st>>>(rkh.ptr, rkl.ptr, n, nl, d, kh.ptr, kl.ptr, bad.ptr);
+    SQD_CHECK_LAUNCH();
+    unsigned long long hbad = 0;
+    copy_to_host(&hbad, bad.ptr, 1, st);
+    if (hbad)
+      throw Error(SQD_ERR_DEVICE, "stored pairs do not follow the product structure (" +
+                                      std::to_string(hbad) + " rows)");
+    L.ho.alloc(nh + 1, st);
+    L.lo.alloc(nl + 1, st);
+    exclusive_scan_i64(kh.ptr, L.ho.ptr, nh, true, st);
+    exclusive_scan_i64(kl.ptr, L.lo.ptr, nl, true, st);
+  }
+  int64_t th = 0, tl = 0;
+  copy_to_host(&th, L.ho.ptr + nh, 1, st);
+  copy_to_host(&tl, L.lo.ptr + nl, 1, st);
+  L.th = th;
+  L.tl = tl;
+  L.hsrc.alloc(std::max<int64_t>(th, 1), st);
+  L.lsrc.alloc(std::max<int64_t>(tl, 1), st);
+  k_hsrc<<<grid_for(nh, 256, 4096), 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, nh, nl, d,
+                                                   L.ho.ptr, L.hsrc.ptr);
+  SQD_CHECK_LAUNCH();
+  k_lsrc<<<grid_for(nl, 256, 4096), 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, nh, nl, d,
+                                                   L.ho.ptr, L.lo.ptr, L.lsrc.ptr);
+  SQD_CHECK_LAUNCH();
+  L.pairs_h = th * nl;
+  L.pairs_l = tl * nh;
+  L.pairs_m = op->nnz - L.pairs_h - L.pairs_l;
+  const int nca = op->value_complex ? 2 : 1;
+  // Panel-major slabs, each panel padded to 32 positions (the padding is never read).
+  const size_t nvh = static_cast<size_t>(std::max<int64_t>(th * ((nl + 31) / 32) * 32, 1)) * nca;
+  const size_t nvl = static_cast<size_t>(std::max<int64_t>(tl * ((nh + 31) / 32) * 32, 1)) * nca;
+  L.vh.alloc(nvh, st);
+  L.vl.alloc(nvl, st);
+  SQD_CUDA(cudaMemsetAsync(L.vh.ptr, 0, nvh * sizeof(double), st));
+  SQD_CUDA(cudaMemsetAsync(L.vl.ptr, 0, nvl * sizeof(double), st));
+  L.vt.alloc(static_cast<size_t>(n) * 2, st);
+  L.tt.alloc(static_cast<size_t>(n) * 2, st);
+  L.t.alloc(L.pairs_m > 0 ? static_cast<size_t>(n) * 2 : 1, st);
+  op->prod = std::move(L);
+  extract(op, st, 1, bad.ptr);
+  unsigned long long hbad = 0;
+  copy_to_host(&hbad, bad.ptr, 1, st);
+  if (hbad) {
+    op->prod = ProductLayout();
+    throw Error(SQD_ERR_DEVICE, "stored sources do not follow the product structure (" +
+                                    std::to_string(hbad) + " pairs)");
+  }
+  if (op->values32.ptr) {
+    to_float(op->prod.vh, op->prod.vh32, st);
+    to_float(op->prod.vl, op->prod.vl32, st);
+  }
+  op->prod.built = 1;
+  SQD_CUDA(cudaStreamSynchronize(st));
+}
+
+// Elements again after a coefficient update (sources unchanged).
+void op_product_values(sqd_op_s* op, cudaStream_t st) {
+  if (!op->prod.built) return;
+  extract(op, st, 0, nullptr);
+  if (op->prod.vh32.ptr) {
+    to_float(op->prod.vh, op->prod.vh32, st);
+    to_float(op->prod.vl, op->prod.vl32, st);
+  }
+}
+
+void op_product_values32(sqd_op_s* op, cudaStream_t st) {
+  if (!op->prod.built || op->prod.vh32.ptr) return;
+  to_float(op->prod.vh, op->prod.vh32, st);
+  to_float(op->prod.vl, op->prod.vl32, st);
+}
+
+void op_product_matvec(sqd_op_s* op, const void* v, void* out, int dtype, cudaStream_t st) {
+  ProductLayout& L = op->prod;
+  const bool dbl = dtype_is_double(dtype);
+  SQD_REQUIRE(dbl || L.vh32.ptr != nullptr, "FP32 product-layout elements were not prepared");
+  const int64_t nh = L.nh, nl = L.nl, n = nh * nl;
+  const int prec = dbl ? 0 : 1;
+  dispatch_vec(dtype, op->value_complex, [&](auto rt, auto ncv_t, auto nca_t) {
+    using R = typename decltype(rt)::type;
+    constexpr int NCV = decltype(ncv_t)::value;
+    constexpr int NCA = decltype(nca_t)::value;
+    using E = std::conditional_t<NCV == 2, std::conditional_t<sizeof(R) == 8, double2, float2>, R>;
+    using ED = std::conditional_t<NCV == 2, double2, double>;
+    const R* vin = static_cast<const R*>(v);
+    R* vout = static_cast<R*>(out);
+    const R* VH;
+    const R* VL;
+    const R* VC;
+    if constexpr (sizeof(R) == 8) {
+      VH = L.vh.ptr;
+      VL = L.vl.ptr;
+      VC = op->values.ptr;
+    } else {
+      VH = L.vh32.ptr;
+      VL = L.vl32.ptr;
+      VC = op->values32.ptr;
+    }
+    R* vt = reinterpret_cast<R*>(L.vt.ptr);
+    // 1. vT[l][h] = v[h][l]
+    launch_transpose<E>(vin, vt, nh, nl, st);
+    // 2. L part: t2[l][h]
+    launch_slab<R, NCV, NCA, false, false>(nl, nh, L.tl, L.lo.ptr, L.lsrc.ptr, VL, vt, nullptr,
+                                           nullptr, nullptr, L.tt.ptr, st);
+    // 3. t2 back in row order, into the vT buffer
+    launch_transpose<ED>(L.tt.ptr, L.vt.ptr, nl, nh, st);
+    // 4. M part: t3[r]
+    if (L.pairs_m > 0) {
+      dispatch_lpr(op->lanes_per_row[prec], [&](auto lpr_t) {
+        constexpr int LPR = decltype(lpr_t)::value;
+        k_mv_mixed<R, NCV, NCA, LPR><<<mixed_grid(n, LPR), 256, 0, st>>>(
+            op->row_ptr.ptr, op->cols.ptr, VC, vin, L.ho.ptr, L.lo.ptr, nl, L.t.ptr, n,
+            op->chunk_rows[prec]);
+        SQD_CHECK_LAUNCH();
+      });
+      // 5. H part plus both partials
+      launch_slab<R, NCV, NCA, true, true>(nh, nl, L.th, L.ho.ptr, L.hsrc.ptr, VH, vin, L.vt.ptr,
+                                           L.t.ptr, vout, nullptr, st);
+    } else {
+      launch_slab<R, NCV, NCA, true, false>(nh, nl, L.th, L.ho.ptr, L.hsrc.ptr, VH, vin,
+                                            L.vt.ptr, nullptr, vout, nullptr, st);
+    }
+  });
+}
+
+}  // namespace sqd
+
+using namespace sqd;
+
+extern "C" int sqd_op_set_layout(sqd_op_t op, int precision, int layout, void* stream) {
+  return guarded([&] {
+    SQD_REQUIRE(op != nullptr, "NULL operator");
+    SQD_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (FP32)");
+    SQD_REQUIRE(layout == SQD_LAYOUT_CSR || layout == SQD_LAYOUT_PRODUCT, "unknown layout");
+    if (layout == SQD_LAYOUT_PRODUCT) {
+      cudaStream_t st = as_stream(stream);
+      op_product_build(op, st);
+      if (precision == 1) {
+        op_ensure_values32(op, st);
+        SQD_CUDA(cudaStreamSynchronize(st));
+      }
+    }
+    op->layout[precision] = layout;
+  });
+}
+
+extern "C" int sqd_op_get_layout(sqd_op_t op, int precision, int* layout) {
+  return guarded([&] {
+    SQD_REQUIRE(op != nullptr && layout != nullptr, "NULL argument");
+    SQD_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (FP32)");
+    *layout = op->layout[precision];
+  });
+}
+
+extern "C" int sqd_op_product_info(sqd_op_t op, void* stream, int64_t* n_high, int64_t* n_low,
+                                   int64_t* pairs_high, int64_t* pairs_low,
+                                   int64_t* pairs_mixed) {
+  return guarded([&] {
+    SQD_REQUIRE(op != nullptr, "NULL operator");
+    int64_t nh = 0, nl = 0, ph = -1, pl = -1, pm = -1;
+    if (op->prod.built) {
+      nh = op->prod.nh;
+      nl = op->prod.nl;
+      ph = op->prod.pairs_h;
+      pl = op->prod.pairs_l;
+      pm = op->prod.pairs_m;
+    } else if (op->x_cache == 1 && op->z_cache == 2) {
+      op_product_detect(op, as_stream(stream), &nh, &nl);
+    }
+    if (n_high) *n_high = nh;
+    if (n_low) *n_low = nl;
+    if (pairs_high) *pairs_high = ph;
+    if (pairs_low) *pairs_low = pl;
+    if (pairs_mixed) *pairs_mixed = pm;
+  });
+}

@@ -215,7 +215,7 @@ extern "C" int sqd_space_create(const uint64_t* states, int64_t n_in, int num_qu
     // Conserved-weight sectors.
     const int h = num_qubits / 2;
     const uint64_t m_all = sp->fill_state;
-    const uint64_t m_lo = (h == 0) ? 0 : ((1ull << h) - 1ull);
+    const uint64_t m_lo = half_mask_low(num_qubits);
     const uint64_t m_hi = m_all & ~m_lo;
     DevBuf<int> stats;
     stats.alloc(6, st);

@@ -194,6 +194,37 @@ class SQDOperator:
         """precision 0: FP64 vectors (float64/complex128), 1: FP32 vectors."""
         _lib.call('sqd_op_set_lanes', self._handle, int(precision), int(lanes))
 
+    LAYOUTS = {'csr': 0, 'product': 1}
+
+    def set_layout(self, precision, layout):
+        """Element layout of the cached matvec for one precision: 'csr' (one pair list per
+        row) or 'product' (dense slabs for the pairs that change one half of the qubits, the
+        other pairs kept in CSR lists).  The product layout needs a product subspace and is
+        built on first use."""
+        _lib.call('sqd_op_set_layout', self._handle, int(precision), self.LAYOUTS[layout],
+                  _lib.stream_ptr())
+
+    def get_layout(self, precision):
+        v = _lib._i32()
+        _lib.call('sqd_op_get_layout', self._handle, int(precision), _lib._c.byref(v))
+        return {k: n for n, k in self.LAYOUTS.items()}[v.value]
+
+    def product_info(self):
+        """{'n_high', 'n_low', 'pairs_high', 'pairs_low', 'pairs_mixed'}; n_high = n_low = 0
+        when the subspace is not a product, pair counts -1 until the slabs are built."""
+        vals = [_lib._i64() for _ in range(5)]
+        _lib.call('sqd_op_product_info', self._handle, _lib.stream_ptr(),
+                  *[_lib._c.byref(v) for v in vals])
+        keys = ('n_high', 'n_low', 'pairs_high', 'pairs_low', 'pairs_mixed')
+        return dict(zip(keys, (v.value for v in vals)))
+
+    @property
+    def has_product_layout(self):
+        """True when the product layout applies (cached elements, product subspace)."""
+        if tuple(self.cache_strategy) != (1, 2):
+            return False
+        return self.product_info()['n_high'] > 0
+
     def matvec(self, v, out=None):
         v = v.contiguous()
         if v.shape[0] != self.size:
@@ -244,17 +275,15 @@ class SQDOperator:
                   _lib.dtype_code(dt), _lib.ptr(out), _lib.stream_ptr())
         return out
 
-    def autotune(self, dtype=None, candidates=(2, 4, 8, 16, 32), reps=5):
-        """Times the matvec for each lanes-per-row choice and keeps the fastest (for the
-        precision of ``dtype``; both precisions when ``dtype`` is None)."""
+    def autotune(self, dtype=None, candidates=(2, 4, 8, 16, 32), reps=5, **kw):
+        """Times the matvec for every schedule (layout, lanes per row, chunk rows) and keeps
+        the fastest, for the precision of ``dtype`` (both precisions when ``dtype`` is None).
+        Extra keywords go to ``autotune.tune_lanes`` (``chunks``, ``layouts``)."""
         from .autotune import tune_lanes
         if dtype is not None:
-            return tune_lanes(self, dtype, candidates, reps)
-        cplx = True
-        return {'fp64': tune_lanes(self, torch.complex128 if cplx else torch.float64,
-                                   candidates, reps),
-                'fp32': tune_lanes(self, torch.complex64 if cplx else torch.float32,
-                                   candidates, reps)}
+            return tune_lanes(self, dtype, candidates, reps, **kw)
+        return {'fp64': tune_lanes(self, torch.complex128, candidates, reps, **kw),
+                'fp32': tune_lanes(self, torch.complex64, candidates, reps, **kw)}
 
 
 def _as_pauli(hamiltonian):

@@ -1,0 +1,150 @@
+"""Product-subspace layout of the cached matvec (dense high-half / low-half slabs plus CSR
+lists for the two-half pairs) against the CSR layout and the CPU oracle (apply_h_x_cached,
+sqd.py:694-709)."""
+import numpy as np
+import pytest
+import torch
+
+import rqutils_b200 as rq
+from rqutils_b200 import workloads as W
+from rqutils_b200._lib import SQDError
+from oracle import symplectic as OS, sqd as OQ
+
+pytestmark = pytest.mark.gpu
+
+# FP64 layouts sum a row in different orders: agreement to a few ulps of the row sums.
+MATVEC_RTOL = 1e-13
+MATVEC32_RTOL = 2e-6
+PREC = {torch.complex128: 0, torch.float64: 0, torch.complex64: 1, torch.float32: 1}
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def _jw_small(seed=0):
+    """JW Hamiltonian of 8 orbitals (16 qubits) on a 24 x 20 product of 3-electron strings."""
+    return W.jw_workload('jw_small', 8, 3, 20, 24, seed)
+
+
+def _oracle_hv(x, z, c, states, n, v, force_real):
+    labels = W.labels_from_xz(x, z, n)
+    oham = OS.from_paulisum((labels, list(c)), force_real=force_real, add_padding=True)
+    sp = OQ.pack_states(OQ.u64_to_states(states, n))
+    xs = np.stack([OQ.get_xsource(xm, sp) for xm in oham.x])
+    return OQ.apply_h_x_cached(v.astype(np.complex128), xs, oham.z, oham.c, sp)
+
+
+def _vector(size, dtype, seed=3):
+    g = torch.Generator().manual_seed(seed)
+    v = torch.randn(size, generator=g, dtype=torch.float64)
+    if dtype.is_complex:
+        v = v + 1j * torch.randn(size, generator=g, dtype=torch.float64)
+    return v.to(dtype).cuda()
+
+
+@pytest.mark.parametrize('dtype', [torch.complex128, torch.complex64, torch.float64,
+                                   torch.float32])
+def test_product_layout_matches_csr_and_oracle(dtype):
+    wl = _jw_small()
+    n = wl.num_qubits
+    ham = rq.PauliSumXZ.from_xz(wl.x, wl.z, wl.coeffs, n, force_real=True, padded=True)
+    op = rq.SQDOperator(ham, rq.Subspace.from_u64(wl.states, n), cache_strategy=(1, 2))
+    info = op.product_info()
+    assert (info['n_high'], info['n_low']) == (24, 20)
+    assert info['pairs_high'] == -1
+    v = _vector(op.size, dtype)
+    prec = PREC[dtype]
+    csr = op.matvec(v).cpu().numpy()
+    ref = _oracle_hv(wl.x, wl.z, wl.coeffs, wl.states, n, v.cpu().numpy(), True)
+    tol = MATVEC_RTOL if prec == 0 else MATVEC32_RTOL
+    op.set_layout(prec, 'product')
+    assert op.get_layout(prec) == 'product' and op.get_layout(1 - prec) == 'csr'
+    info = op.product_info()
+    assert info['pairs_high'] + info['pairs_low'] + info['pairs_mixed'] == op.nnz
+    assert min(info['pairs_high'], info['pairs_low'], info['pairs_mixed']) > 0
+    for lanes in (1, 4, 32):
+        for chunk in (0, 64):
+            op.set_lanes(prec, lanes)
+            op.set_chunk(prec, chunk)
+            got = op.matvec(v).cpu().numpy()
+            assert rel(got, ref) < tol
+            assert rel(got, csr) < (MATVEC_RTOL if prec == 0 else MATVEC32_RTOL)
+
+
+@pytest.mark.parametrize('dtype', [torch.complex128, torch.complex64])
+def test_product_layout_complex_elements(dtype):
+    rng = np.random.default_rng(11)
+    x, z, c = W.random_pauli_sum(16, 500, rng, wmax=4)
+    states = W.product_subspace(8, 4, 30, 22, rng)
+    ham = rq.PauliSumXZ.from_xz(x, z, c, 16, padded=True)
+    op = rq.SQDOperator(ham, rq.Subspace.from_u64(states, 16), cache_strategy=(1, 2))
+    assert op.value_complex
+    v = _vector(op.size, dtype, seed=5)
+    ref = _oracle_hv(x, z, c, states, 16, v.cpu().numpy(), False)
+    op.set_layout(PREC[dtype], 'product')
+    got = op.matvec(v).cpu().numpy()
+    assert rel(got, ref) < (MATVEC_RTOL if PREC[dtype] == 0 else MATVEC32_RTOL)
+
+
+def test_product_layout_without_two_half_pairs_or_diagonal():
+    """Terms on one half only (no two-half pairs) and no Z-only group (no diagonal entry)."""
+    rng = np.random.default_rng(4)
+    xl, zl, cl = W.random_pauli_sum(8, 60, rng, wmin=1, wmax=3)
+    xh, zh, ch = W.random_pauli_sum(8, 60, rng, wmin=1, wmax=3)
+    keep_l, keep_h = xl != 0, xh != 0
+    x = np.concatenate([xl[keep_l], xh[keep_h] << np.uint64(8)])
+    z = np.concatenate([zl[keep_l], zh[keep_h] << np.uint64(8)])
+    c = np.concatenate([cl[keep_l], ch[keep_h]])
+    states = W.product_subspace(8, 4, 25, 33, rng)
+    ham = rq.PauliSumXZ.from_xz(x, z, c, 16, force_real=True, padded=True)
+    op = rq.SQDOperator(ham, rq.Subspace.from_u64(states, 16), cache_strategy=(1, 2))
+    v = _vector(op.size, torch.complex128, seed=9)
+    ref = _oracle_hv(x, z, c, states, 16, v.cpu().numpy(), True)
+    for prec, dt in ((0, torch.complex128), (1, torch.complex64)):
+        op.set_layout(prec, 'product')
+        got = op.matvec(v.to(dt)).cpu().numpy()
+        assert rel(got, ref) < (MATVEC_RTOL if prec == 0 else MATVEC32_RTOL)
+    assert op.product_info()['pairs_mixed'] == 0
+
+
+def test_product_layout_rejected_for_other_subspaces():
+    wl = W.c1(0)                                   # weight-8 strings: not a product
+    ham = rq.PauliSumXZ.from_xz(wl.x, wl.z, wl.coeffs, 16, force_real=True, padded=True)
+    op = rq.SQDOperator(ham, rq.Subspace.from_u64(wl.states, 16), cache_strategy=(1, 2))
+    assert op.product_info()['n_high'] == 0 and not op.has_product_layout
+    with pytest.raises(SQDError):
+        op.set_layout(0, 'product')
+    assert op.get_layout(0) == 'csr'
+    # a product subspace with fill-in slots is refused too
+    jw = _jw_small()
+    hj = rq.PauliSumXZ.from_xz(jw.x, jw.z, jw.coeffs, 16, force_real=True, padded=True)
+    sp = rq.Subspace.from_u64(jw.states, 16, states_size=jw.states.shape[0] + 7)
+    opf = rq.SQDOperator(hj, sp, cache_strategy=(1, 2))
+    with pytest.raises(SQDError):
+        opf.set_layout(0, 'product')
+    # uncached elements: no product layout
+    opx = rq.SQDOperator(hj, rq.Subspace.from_u64(jw.states, 16), cache_strategy=(1, 0))
+    assert not opx.has_product_layout
+
+
+def test_product_layout_locg_autotune_and_refresh():
+    wl = _jw_small(1)
+    n = wl.num_qubits
+    ham = rq.PauliSumXZ.from_xz(wl.x, wl.z, wl.coeffs, n, force_real=True, padded=True)
+    op = rq.SQDOperator(ham, rq.Subspace.from_u64(wl.states, n), cache_strategy=(1, 2))
+    x0 = torch.as_tensor(wl.start_vector(), device='cuda')
+    e_csr, _, _ = rq.ground_locg(op, x0, mode='fp64')
+    tuned = op.autotune(layouts=('product',))
+    assert tuned['fp64']['layout'] == 'product' and tuned['fp32']['layout'] == 'product'
+    for mode in ('fp64', 'mixed'):
+        e, _, _ = rq.ground_locg(op, x0, mode=mode)
+        assert abs(e - e_csr) <= 1e-10 * abs(e_csr)
+    # coefficient update: the slabs follow the refreshed elements
+    c2 = wl.coeffs * 1.3
+    ham.set_coeffs(torch.as_tensor(c2))
+    op.refresh()
+    v = _vector(op.size, torch.complex128, seed=2)
+    ref = _oracle_hv(wl.x, wl.z, c2, wl.states, n, v.cpu().numpy(), True)
+    assert rel(op.matvec(v).cpu().numpy(), ref) < MATVEC_RTOL
+    assert rel(op.matvec(v.to(torch.complex64)).cpu().numpy(), ref) < MATVEC32_RTOL

@@ -60,3 +60,14 @@ def test_workload_generators_are_seeded_and_shaped():
     assert st.shape[0] == 20 and (np.diff(st.astype(np.float64)) > 0).all()
     aa, bb = W.c4_dims(0)
     assert aa.shape == (96,) and aa.min() >= 64 and bb.max() <= 1820
+
+
+def test_every_package_module_imports():
+    """Lazily imported modules (autotune, autograd, batched, ...) must at least import."""
+    import importlib
+    import pkgutil
+    import rqutils_b200
+    names = [m.name for m in pkgutil.walk_packages(rqutils_b200.__path__, 'rqutils_b200.')]
+    assert 'rqutils_b200.autotune' in names
+    for name in names:
+        importlib.import_module(name)
