@@ -84,6 +84,12 @@ struct ProductLayout {
   sqd::DevBuf<double> vt, tt, t;     // per-matvec scratch: transposed input, L and M partials
 };
 
+// Solver objects an operator keeps between LOCG solves (locg.cu): work vectors and the
+// instantiated CUDA graphs of the iteration, rebuilt when the matvec schedule changes.
+struct LocgCacheBase {
+  virtual ~LocgCacheBase() = default;
+};
+
 struct sqd_op_s {
   sqd_paulis_s* p = nullptr;   // borrowed: must outlive the operator
   sqd_space_s* s = nullptr;    // borrowed
@@ -103,6 +109,10 @@ struct sqd_op_s {
   sqd::DevBuf<int> status;        // device status word
   int layout[2] = {0, 0};         // SQD_LAYOUT_* per precision
   ProductLayout prod;
+  // Bumped whenever the kernels or buffers a matvec launches may change (lanes, chunk,
+  // layout, coefficient refresh): cached solver graphs captured before are then stale.
+  uint64_t schedule_version = 0;
+  std::unique_ptr<LocgCacheBase> locg_cache;
 };
 
 namespace sqd {

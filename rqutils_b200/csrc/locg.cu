@@ -19,6 +19,8 @@
 #include "dispatch.cuh"
 #include "accum.cuh"
 
+#include <tuple>
+
 namespace sqd {
 namespace {
 
@@ -510,6 +512,171 @@ __global__ void __launch_bounds__(LC_THREADS) k_lc(LCArgs<MAXS, MAXD, MAXO> a) {
   }
 }
 
+// A pass whose shape is known at compile time: NS sources, NO outputs and the dots' operand
+// codes (k < NS: source k; 100 + q: output q).  The generic k_lc reads these from its
+// arguments and predicates every unrolled step and operand choice on them, which makes its
+// widest form instruction-bound; the hot passes of the LOCG iterations run through this
+// specialisation instead (same arguments, same post-op, same deterministic reduction).
+template <int NS_, int NO_, int... D>
+struct PassShape {
+  static constexpr int NS = NS_, NO = NO_, ND = int(sizeof...(D)) / 2;
+  static constexpr int codes[sizeof...(D) + 2] = {D..., 0, 0};
+};
+
+template <int C, int NO>
+__device__ __forceinline__ double2 operand(const double2* s, const double2* o) {
+  if constexpr (C >= 100) return o[C - 100];
+  else return s[C];
+}
+
+template <typename S, int I, int END>
+struct DotLoop {
+  __device__ __forceinline__ static void run(double (*acc)[2], const double2* s, const double2* o) {
+    if constexpr (I < END) {
+      const double2 x = operand<S::codes[2 * I], S::NO>(s, o);
+      const double2 y = operand<S::codes[2 * I + 1], S::NO>(s, o);
+      acc[I][0] += x.x * y.x + x.y * y.y;   // conj(x) * y
+      acc[I][1] += x.x * y.y - x.y * y.x;
+      DotLoop<S, I + 1, END>::run(acc, s, o);
+    }
+  }
+};
+
+template <typename R, int NC, typename S>
+__global__ void __launch_bounds__(LC_THREADS) k_lcs(LCArgs<6, 10, 5> a) {
+  constexpr int NS = S::NS, NO = S::NO, ND = S::ND;
+  constexpr int NOA = NO > 0 ? NO : 1, NDA = ND > 0 ? ND : 1;
+  LocgDev* dev = a.dev;
+  if ((a.gate & G_DONE) && *(volatile int*)&dev->done) return;
+  if ((a.gate & G_KEEP) && *(volatile int*)&dev->keep) return;
+  __shared__ double2 sc[NOA][NS];
+  for (int t = threadIdx.x; t < NO * NS; t += blockDim.x)
+    sc[t / NS][t % NS] = make_double2(dev->coef[t / NS][t % NS][0], dev->coef[t / NS][t % NS][1]);
+  __syncthreads();
+  double acc[NDA][2];
+#pragma unroll
+  for (int d = 0; d < NDA; ++d) acc[d][0] = acc[d][1] = 0.0;
+  // One element per thread per step (U > 1 makes the compiler keep every coefficient of the
+  // wide shapes in registers; they then spill).
+  constexpr int U = 1;
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i0 = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i0 < a.n; i0 += U * stride) {
+    Cx<R> raw[U][NS];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = i0 + u * stride;
+#pragma unroll
+      for (int k = 0; k < NS; ++k)
+        raw[u][k] = i < a.n ? ld_elem_rw<R, NC>(static_cast<const R*>(a.src[k]), i)
+                            : cx_make<R>(R(0), R(0));
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = i0 + u * stride;
+      double2 sv[NS];
+#pragma unroll
+      for (int k = 0; k < NS; ++k) sv[k] = make_double2(double(raw[u][k].re), double(raw[u][k].im));
+      double2 ov[NOA];
+#pragma unroll
+      for (int q = 0; q < NO; ++q) {
+        double2 t = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int k = 0; k < NS; ++k) t = cadd(t, cmul(sc[q][k], sv[k]));
+        if constexpr (NC == 1) t.y = 0.0;
+        ov[q] = t;
+      }
+      if (i < a.n) {
+        DotLoop<S, 0, ND>::run(acc, sv, ov);
+#pragma unroll
+        for (int q = 0; q < NO; ++q)
+          if (a.out[q] != nullptr)
+            st_elem<R, NC>(static_cast<R*>(a.out[q]), i, cx_make<R>(R(ov[q].x), R(ov[q].y)));
+      }
+    }
+  }
+  if (ND == 0 && a.post == P_NONE) return;
+  __shared__ double sred[NDA * 2][LC_THREADS / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    const double v0 = warp_sum(acc[d][0]);
+    const double v1 = warp_sum(acc[d][1]);
+    if (lane == 0) {
+      sred[2 * d][warp] = v0;
+      sred[2 * d + 1][warp] = v1;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * ND) {
+    double t = 0.0;
+    for (int w = 0; w < LC_THREADS / 32; ++w) t += sred[threadIdx.x][w];
+    a.partials[static_cast<int64_t>(blockIdx.x) * (2 * 10) + threadIdx.x] = t;
+  }
+  __threadfence();
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(a.counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x < 2 * ND) {
+    double t = 0.0;
+    for (unsigned b = 0; b < gridDim.x; ++b)
+      t += *(volatile double*)&a.partials[static_cast<int64_t>(b) * (2 * 10) + threadIdx.x];
+    dev->red[threadIdx.x >> 1][threadIdx.x & 1] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    run_post(dev, a.post, a.nsrc, a.use_cond, a.cond);
+    *a.counter = 0u;
+  }
+}
+
+// The pass shapes of the LOCG iterations (reference body, fast implicit body, start/refresh).
+using ShapeList = std::tuple<
+    PassShape<3, 1, 100, 100, 1, 100, 2, 100>,               // project + normalise + ips
+    PassShape<3, 1>,                                         // p = combination of (p, x, y)
+    PassShape<6, 0, 0, 3, 1, 4, 2, 5, 1, 3, 2, 3, 2, 4, 2, 2, 1, 2>,  // implicit Gram
+    PassShape<6, 4, 100, 100, 101, 101>,                     // x, y, Ax, Ay and norms
+    PassShape<4, 5, 104, 104, 102, 102, 100, 104, 101, 104>, // scale, residual, next ips
+    PassShape<3, 0, 1, 0, 2, 0>,                             // <x|r>, <y|r>
+    PassShape<3, 1, 1, 100, 2, 100>,
+    PassShape<3, 1, 100, 100>,
+    PassShape<1, 1>,
+    PassShape<6, 0, 0, 3, 1, 4, 2, 5, 1, 3, 2, 3, 2, 4>,     // reference Gram (3x3)
+    PassShape<3, 2, 100, 100, 101, 101>,
+    PassShape<2, 2>,
+    PassShape<2, 1, 100, 100, 0, 0>,                         // residual + convergence
+    PassShape<2, 1, 0, 0>,
+    PassShape<1, 0, 0, 0>,
+    PassShape<2, 0, 1, 0>,
+    PassShape<2, 1, 100, 100>,
+    PassShape<4, 0, 0, 2, 1, 2, 1, 3>,
+    PassShape<2, 2, 100, 100, 101, 101>>;
+
+template <typename S>
+bool shape_matches(const LCArgs<6, 10, 5>& a) {
+  if (a.nsrc != S::NS || a.nout != S::NO || a.ndot != S::ND) return false;
+  for (int d = 0; d < S::ND; ++d)
+    if (a.da[d] != S::codes[2 * d] || a.db[d] != S::codes[2 * d + 1]) return false;
+  return true;
+}
+
+// Launches the specialised pass for a's shape; false when no listed shape matches.
+template <typename R, int NC, size_t I = 0>
+bool launch_shaped(const LCArgs<6, 10, 5>& a, unsigned blocks, cudaStream_t st) {
+  if constexpr (I < std::tuple_size<ShapeList>::value) {
+    using S = std::tuple_element_t<I, ShapeList>;
+    if (shape_matches<S>(a)) {
+      k_lcs<R, NC, S><<<blocks, LC_THREADS, 0, st>>>(a);
+      return true;
+    }
+    return launch_shaped<R, NC, I + 1>(a, blocks, st);
+  } else {
+    return false;
+  }
+}
+
 template <typename R, int NC>
 __global__ void k_onehot(R* x, int64_t n, int64_t idx) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
@@ -562,6 +729,9 @@ class Locg {
 
   R* x() { return x_.ptr; }
   LocgDev* dev() { return dev_.ptr; }
+  // A cached solver serving a later call on another stream (its previous work has finished:
+  // every solve ends with a stream synchronisation).
+  void set_stream(cudaStream_t st) { st_ = cur_ = st; }
 
   void set_params(double tol, double nscale, int maxiter, double inner_rtol, double etol,
                   int stall) {
@@ -581,6 +751,14 @@ class Locg {
   // ---- one fused pass
   void lc(std::initializer_list<const void*> srcs, std::initializer_list<void*> outs,
           std::initializer_list<std::pair<int, int>> dots, int post, int gate = G_NONE) {
+    if (srcs.size() <= 6 && dots.size() <= 10 && outs.size() <= 5) {
+      Wide w{};
+      fill(w, srcs, outs, dots, post, gate);
+      if (launch_shaped<R, NC>(w, blocks_, cur_)) {
+        SQD_CHECK_LAUNCH();
+        return;
+      }
+    }
     if (srcs.size() <= 3 && dots.size() <= 3 && outs.size() <= 2) {
       Tiny a{};
       fill(a, srcs, outs, dots, post, gate);
@@ -932,16 +1110,60 @@ int op_cb64(void* ctx, const void* x, void* y, void* stream) {
   return guarded([&] { op_matvec(c->op, x, y, c->dtype, as_stream(stream)); });
 }
 
+// Solver objects kept on the operator between solves: the work vectors and the instantiated
+// graphs of the iteration loops are reused instead of allocated and captured again (the first
+// FP64 phase after the FP32 sweeps otherwise waits for the pool to map 8 new vectors).
+// Valid while n, the vector kind and the operator's matvec schedule stay the same; only solves
+// without orthogonality constraints use it (a captured graph holds the constraint vectors).
 template <int NC>
-void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xinit,
-              int64_t xinit_index, const std::vector<const void*>& orth, double tol,
-              int maxiter, int mode, bool use_graph, cudaStream_t st, double* eigval,
-              void* eigvec, int* niter, double* residual) {
+struct SolverCache final : LocgCacheBase {
+  int64_t n = 0;
+  uint64_t version = 0;
+  OpCtx32 c32{};
+  OpCtx64 c64{};
+  std::unique_ptr<Locg<float, NC>> l32;
+  std::unique_ptr<Locg<double, NC>> l64;
+};
+
+template <int NC>
+SolverCache<NC>* solver_cache(sqd_op_s* op, int64_t n) {
+  auto* c = dynamic_cast<SolverCache<NC>*>(op->locg_cache.get());
+  if (!c || c->n != n || c->version != op->schedule_version) {
+    op->locg_cache.reset();  // frees the stale objects first
+    auto fresh = std::make_unique<SolverCache<NC>>();
+    fresh->n = n;
+    fresh->version = op->schedule_version;
+    fresh->c32 = OpCtx32{op, NC == 2 ? SQD_C64 : SQD_F32};
+    fresh->c64 = OpCtx64{op, NC == 2 ? SQD_C128 : SQD_F64};
+    c = fresh.get();
+    op->locg_cache = std::move(fresh);
+  }
+  return c;
+}
+
+// cache_op: the sqd operator behind fn (NULL for a caller's own matvec), whose solver cache
+// the FP64 path may use.
+template <int NC>
+void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, sqd_op_s* cache_op,
+              const void* xinit, int64_t xinit_index, const std::vector<const void*>& orth,
+              double tol, int maxiter, int mode, bool use_graph, cudaStream_t st,
+              double* eigval, void* eigvec, int* niter, double* residual) {
   const double eps64 = 2.220446049250313e-16;
   const double nscale = 10.0 * static_cast<double>(n);
   const unsigned G = grid_for(n, 256, 8192);
   if (mode == SQD_LOCG_FP64) {
-    Locg<double, NC> L(n, fn, ctx, st);
+    std::unique_ptr<Locg<double, NC>> own;
+    Locg<double, NC>* lp = nullptr;
+    if (cache_op && orth.empty()) {
+      auto* cache = solver_cache<NC>(cache_op, n);
+      if (!cache->l64) cache->l64 = std::make_unique<Locg<double, NC>>(n, op_cb64, &cache->c64, st);
+      lp = cache->l64.get();
+      lp->set_stream(st);
+    } else {
+      own = std::make_unique<Locg<double, NC>>(n, fn, ctx, st);
+      lp = own.get();
+    }
+    Locg<double, NC>& L = *lp;
     L.set_params(tol < 0 ? eps64 : tol, nscale, maxiter, 0.0, 0.0, 0);
     if (xinit)
       SQD_CUDA(cudaMemcpyAsync(L.x(), xinit, sizeof(double) * NC * n, cudaMemcpyDeviceToDevice,
@@ -972,11 +1194,10 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xin
   SQD_REQUIRE(fn == sqd_op_matvec_cb, "mixed precision needs an sqd operator as the matvec");
   auto* op = static_cast<sqd_op_s*>(ctx);
   op_ensure_values32(op, st);
-  OpCtx32 c32{op, NC == 2 ? SQD_C64 : SQD_F32};
-  OpCtx64 c64{op, NC == 2 ? SQD_C128 : SQD_F64};
+  SolverCache<NC>* cache = solver_cache<NC>(op, n);
   // Phase timing on stderr when SQD_LOCG_TRACE is set (like the reference's debug prints).
   const bool trace = std::getenv("SQD_LOCG_TRACE") != nullptr;
-  cudaEvent_t ev[4] = {};
+  cudaEvent_t ev[5] = {};
   if (trace)
     for (auto& e : ev) SQD_CUDA(cudaEventCreate(&e));
   auto mark = [&](int k) {
@@ -987,52 +1208,53 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xin
   constexpr int kStall = 25;
   constexpr int kRestarts = 6;
   int it32 = 0;
-  DevBuf<double> x64;
-  x64.alloc(static_cast<size_t>(n) * NC, st);
+  if (!cache->l64) cache->l64 = std::make_unique<Locg<double, NC>>(n, op_cb64, &cache->c64, st);
+  Locg<double, NC>& L = *cache->l64;
+  L.set_stream(st);
   {
-    Locg<float, NC> L(n, op_cb32, &c32, st);
-    L.set_params(0.0, nscale, maxiter, kInnerRtol, 0.0, kStall);
+    if (!cache->l32) cache->l32 = std::make_unique<Locg<float, NC>>(n, op_cb32, &cache->c32, st);
+    Locg<float, NC>& L32 = *cache->l32;
+    L32.set_stream(st);
+    L32.set_params(0.0, nscale, maxiter, kInnerRtol, 0.0, kStall);
     if (xinit) {
-      k_convert<float, double, NC><<<G, 256, 0, st>>>(static_cast<const double*>(xinit), L.x(),
-                                                     n);
+      k_convert<float, double, NC><<<G, 256, 0, st>>>(static_cast<const double*>(xinit),
+                                                     L32.x(), n);
     } else {
-      k_onehot<float, NC><<<G, 256, 0, st>>>(L.x(), n, xinit_index);
+      k_onehot<float, NC><<<G, 256, 0, st>>>(L32.x(), n, xinit_index);
     }
     SQD_CHECK_LAUNCH();
-    L.start_implicit();
-    L.proj_ips();
+    L32.start_implicit();
+    L32.proj_ips();
     for (int k = 0; k < kRestarts; ++k) {
-      L.loop(orth, maxiter, use_graph, true);
-      if (L.host().niter >= maxiter || L.host().rzero) break;
-      L.refresh();
-      if (L.host().converged || L.host().niter >= maxiter) break;
+      L32.loop(orth, maxiter, use_graph, true);
+      if (L32.host().niter >= maxiter || L32.host().rzero) break;
+      L32.refresh();
+      if (L32.host().converged || L32.host().niter >= maxiter) break;
     }
-    it32 = L.host().niter;
-    k_convert<double, float, NC><<<G, 256, 0, st>>>(L.x(), x64.ptr, n);
+    it32 = L32.host().niter;
+    k_convert<double, float, NC><<<G, 256, 0, st>>>(L32.x(), L.x(), n);
     SQD_CHECK_LAUNCH();
     mark(1);
   }
   // FP64 polish: fast implicit iterations (one FP64 matvec each) with the reference's
   // residual test; in FP64 the carried products drift by O(eps) only.
-  Locg<double, NC> L(n, op_cb64, &c64, st);
+  mark(2);
   const int left = std::max(1, maxiter - it32);
   L.set_params(tol < 0 ? eps64 : tol, nscale, left, 0.0, 0.0, 0);
-  SQD_CUDA(cudaMemcpyAsync(L.x(), x64.ptr, sizeof(double) * NC * n, cudaMemcpyDeviceToDevice,
-                           st));
   L.start_implicit();
   L.proj_ips();
-  mark(2);
+  mark(3);
   L.loop(orth, left, use_graph, true);
   const int it64 = L.host().niter;
-  mark(3);
+  mark(4);
   if (trace) {
-    SQD_CUDA(cudaEventSynchronize(ev[3]));
-    float t[3];
-    for (int k = 0; k < 3; ++k) SQD_CUDA(cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]));
+    SQD_CUDA(cudaEventSynchronize(ev[4]));
+    float t[4];
+    for (int k = 0; k < 4; ++k) SQD_CUDA(cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]));
     std::fprintf(stderr,
-                 "[sqd_locg mixed] fp32 sweeps %d it %.3f ms | fp64 start %.3f ms | "
-                 "fp64 iterations %d it %.3f ms\n",
-                 it32, t[0], t[1], it64, t[2]);
+                 "[sqd_locg mixed] fp32 sweeps %d it %.3f ms | phase switch %.3f ms | "
+                 "fp64 start %.3f ms | fp64 iterations %d it %.3f ms\n",
+                 it32, t[0], t[1], t[2], it64, t[3]);
     for (auto& e : ev) cudaEventDestroy(e);
   }
   const LocgDev& h = L.host();
@@ -1634,11 +1856,11 @@ extern "C" int sqd_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const
       graph = false;  // foreign callbacks may synchronise; no capture
     }
     if (dtype == SQD_C128)
-      run_locg<2>(n, dtype, f, c, xinit, xinit_index, ov, tol, maxiter, mode, graph, st,
-                  eigval_host, eigvec, niter_host, residual_host);
+      run_locg<2>(n, dtype, f, c, octx.op, xinit, xinit_index, ov, tol, maxiter, mode, graph,
+                  st, eigval_host, eigvec, niter_host, residual_host);
     else
-      run_locg<1>(n, dtype, f, c, xinit, xinit_index, ov, tol, maxiter, mode, graph, st,
-                  eigval_host, eigvec, niter_host, residual_host);
+      run_locg<1>(n, dtype, f, c, octx.op, xinit, xinit_index, ov, tol, maxiter, mode, graph,
+                  st, eigval_host, eigvec, niter_host, residual_host);
   });
 }
 

@@ -497,6 +497,7 @@ extern "C" int sqd_op_set_lanes(sqd_op_t op, int precision, int lanes_per_row) {
     SQD_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (FP32)");
     dispatch_lpr(lanes_per_row, [](auto) {});
     op->lanes_per_row[precision] = lanes_per_row;
+    ++op->schedule_version;
   });
 }
 
@@ -506,6 +507,7 @@ extern "C" int sqd_op_set_chunk(sqd_op_t op, int precision, int64_t chunk_rows) 
     SQD_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (FP32)");
     SQD_REQUIRE(chunk_rows >= 0, "chunk_rows must be >= 0");
     op->chunk_rows[precision] = chunk_rows;
+    ++op->schedule_version;
   });
 }
 
@@ -642,6 +644,7 @@ extern "C" int sqd_op_refresh(sqd_op_t op, void* stream) {
       SQD_CHECK_LAUNCH();
     }
     op_product_values(op, st);
+    ++op->schedule_version;
   });
 }
 

@@ -556,6 +556,7 @@ extern "C" int sqd_op_set_layout(sqd_op_t op, int precision, int layout, void* s
       }
     }
     op->layout[precision] = layout;
+    ++op->schedule_version;
   });
 }
 

@@ -1,0 +1,58 @@
+"""Solver objects cached on an operator between LOCG solves: repeated solves, solves after a
+change of the matvec schedule or of the coefficients, and solves on another stream must give
+the results of a fresh operator."""
+import numpy as np
+import pytest
+import torch
+
+import rqutils_b200 as rq
+from rqutils_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(seed=2):
+    wl = W.jw_workload('jw_small', 8, 3, 20, 24, seed)
+    ham = rq.PauliSumXZ.from_xz(wl.x, wl.z, wl.coeffs, wl.num_qubits, force_real=True,
+                                padded=True)
+    space = rq.Subspace.from_u64(wl.states, wl.num_qubits)
+    return wl, ham, space
+
+
+@pytest.mark.parametrize('mode', ['fp64', 'mixed'])
+def test_repeated_solves_reuse_and_stay_exact(mode):
+    wl, ham, space = _case()
+    op = rq.SQDOperator(ham, space, cache_strategy=(1, 2))
+    x0 = torch.as_tensor(wl.start_vector(), device='cuda')
+    e1, v1, it1 = rq.ground_locg(op, x0, mode=mode)
+    e2, v2, it2 = rq.ground_locg(op, x0, mode=mode)
+    assert e1 == e2 and it1 == it2                      # deterministic reductions, same path
+    torch.testing.assert_close(v1, v2, rtol=0, atol=0)
+    # schedule changes between solves: the cached graphs are rebuilt
+    op.set_lanes(0, 4)
+    op.set_lanes(1, 8)
+    op.set_layout(0, 'product')
+    op.set_layout(1, 'product')
+    e3, _, _ = rq.ground_locg(op, x0, mode=mode)
+    assert abs(e3 - e1) <= 1e-12 * abs(e1)
+    # another stream
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        e4, _, _ = rq.ground_locg(op, x0, mode=mode)
+    torch.cuda.synchronize()
+    assert abs(e4 - e1) <= 1e-12 * abs(e1)
+
+
+def test_cached_solver_follows_coefficient_refresh():
+    wl, ham, space = _case(5)
+    op = rq.SQDOperator(ham, space, cache_strategy=(1, 2))
+    x0 = torch.as_tensor(wl.start_vector(), device='cuda')
+    rq.ground_locg(op, x0, mode='mixed')
+    c2 = wl.coeffs * 0.8 + 0.01 * np.sign(wl.coeffs)
+    ham.set_coeffs(torch.as_tensor(c2))
+    op.refresh()
+    e_cached, _, _ = rq.ground_locg(op, x0, mode='mixed')
+    fresh = rq.SQDOperator(rq.PauliSumXZ.from_xz(wl.x, wl.z, c2, wl.num_qubits, force_real=True,
+                                                 padded=True), space, cache_strategy=(1, 2))
+    e_fresh, _, _ = rq.ground_locg(fresh, x0, mode='mixed')
+    assert abs(e_cached - e_fresh) <= 1e-12 * abs(e_fresh)
