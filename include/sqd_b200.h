@@ -198,7 +198,11 @@ enum sqd_locg_mode {
  *  tol < 0 selects the dtype epsilon (:224-225).
  *  use_graph: capture each iteration in a CUDA graph (only with fn == sqd_op_matvec_cb).
  *  Outputs: eigval_host, eigvec (device, n elements of dtype), niter_host, and
- *  residual_host = final |r| (may be NULL). */
+ *  residual_host = final |r| (may be NULL).
+ *  With an sqd_op_t and no orth vectors, the solver's work vectors and captured iteration
+ *  graphs stay with the operator for its next solve (no rqutils counterpart: XLA caches its
+ *  compiled loop per shape): 8 vectors of dtype, plus 8 FP32 ones after a mixed solve, held
+ *  until sqd_op_destroy; they are rebuilt when lanes, chunk, layout or coefficients change. */
 int sqd_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xinit,
              int64_t xinit_index, const void* const* orth, int n_orth, double tol, int maxiter,
              int mode, int use_graph, void* stream, double* eigval_host, void* eigvec,
