@@ -48,7 +48,7 @@ def parse():
     ap.add_argument('--cpu-rows', type=int, default=0, help='CPU sample rows (0 = auto)')
     ap.add_argument('--lanes', type=int, default=0, help='lanes per row (0 = autotune)')
     ap.add_argument('--chunk', type=int, default=0, help='rows per block chunk with --lanes')
-    ap.add_argument('--layout', default='csr', choices=['csr', 'product'],
+    ap.add_argument('--layout', default='csr', choices=['csr', 'product', 'product-csr'],
                     help='element layout with --lanes (the autotuner picks it otherwise)')
     return ap.parse_args()
 
@@ -310,7 +310,7 @@ def run_ours(args):
     # two-half CSR tails (when there are any), high-half slabs
     layout = op.get_layout(0) if cache == (1, 2) else 'csr'
     per_step = 1
-    if layout == 'product':
+    if layout in ('product', 'product-csr'):
         per_step = 5 if op.product_info()['pairs_mixed'] > 0 else 4
     gpu_launches = args.steps * per_step
 

@@ -132,11 +132,13 @@ int sqd_op_set_chunk(sqd_op_t op, int precision, int64_t chunk_rows);
  * that is the product of strings on the high and the low half of the qubits (every high string
  * with every low string, no fill-in slots), the pairs that change one half only are stored as
  * dense slabs whose sources are implied by their position (coalesced loads, no index per
- * pair); the pairs that change both halves keep their CSR lists (lanes and chunk knobs apply
- * to those).  Setting SQD_LAYOUT_PRODUCT builds the slabs on first use (SQD_ERR_UNSUPPORTED
- * when the subspace is not such a product); results equal the CSR layout's up to the order of
- * each row's sum. */
-enum sqd_layout { SQD_LAYOUT_CSR = 0, SQD_LAYOUT_PRODUCT = 1 };
+ * pair); the pairs that change both halves gather from their source slabs staged in shared
+ * memory when all of a slab's sources fit there, else from their CSR lists.
+ * SQD_LAYOUT_PRODUCT_CSR: the same slabs, with the two-half pairs always on the CSR lists.
+ * Lanes and chunk knobs apply to the two-half pairs.  Setting a product layout builds the
+ * slabs on first use (SQD_ERR_UNSUPPORTED when the subspace is not such a product); results
+ * equal the CSR layout's up to the order of each row's sum. */
+enum sqd_layout { SQD_LAYOUT_CSR = 0, SQD_LAYOUT_PRODUCT = 1, SQD_LAYOUT_PRODUCT_CSR = 2 };
 int sqd_op_set_layout(sqd_op_t op, int precision, int layout, void* stream);
 int sqd_op_get_layout(sqd_op_t op, int precision, int* layout);
 /* Product structure: n_high x n_low rows (0, 0 when the subspace is not a product) and, once

@@ -29,15 +29,15 @@ def _time(fn, reps):
 def tune_lanes(op, dtype, candidates=(2, 4, 8, 16, 32), reps=5, chunks=(0, 64, 256, 1024),
                layouts=None):
     """Times every (layout, lanes per row, chunk rows) schedule of the cached matvec for the
-    precision of ``dtype`` and keeps the fastest.  ``layouts`` defaults to 'csr' plus
-    'product' when that layout applies (its lanes and chunks schedule the two-half pairs)."""
+    precision of ``dtype`` and keeps the fastest.  ``layouts`` defaults to 'csr' plus the
+    product layouts when they apply (their lanes and chunks schedule the two-half pairs)."""
     if op.cache_strategy[0] != 1:
         return {'lanes_per_row': None, 'note': 'uncached matvec has a fixed schedule'}
     if op.value_complex and not dtype.is_complex:
         dtype = torch.complex128 if dtype == torch.float64 else torch.complex64
     precision = 0 if dtype in (torch.float64, torch.complex128) else 1
     if layouts is None:
-        layouts = ('csr', 'product') if op.has_product_layout else ('csr',)
+        layouts = ('csr', 'product', 'product-csr') if op.has_product_layout else ('csr',)
     key = (op.size, op.nnz, op.cache_strategy, dtype, tuple(layouts))
     if key in _CACHE:
         best = _CACHE[key]

@@ -82,6 +82,16 @@ struct ProductLayout {
   sqd::DevBuf<double> vh, vl;        // FP64 elements (x2 interleaved when complex)
   sqd::DevBuf<float> vh32, vl32;     // FP32 copies
   sqd::DevBuf<double> vt, tt, t;     // per-matvec scratch: transposed input, L and M partials
+  // M pairs gathered from shared memory, built when every slab's M source slabs fit there
+  // together: compact copies of the row tails (mptr, mval) whose sources are indices into the
+  // block's staged slabs (msidx = slot * nl + l'), and each slab's source slabs (slist).
+  int tail_slots = 0;                // largest number of M source slabs of one slab
+  sqd::DevBuf<int64_t> mptr;         // [n + 1]
+  sqd::DevBuf<uint16_t> msidx;       // [pairs_m]
+  sqd::DevBuf<double> mval;          // [pairs_m] (x2 interleaved when complex)
+  sqd::DevBuf<float> mval32;
+  sqd::DevBuf<int64_t> soff;         // [nh + 1]
+  sqd::DevBuf<uint32_t> slist;       // [soff[nh]] ascending source slabs
 };
 
 // Solver objects an operator keeps between LOCG solves (locg.cu): work vectors and the

@@ -15,7 +15,7 @@
 //   1. vT = transpose(v)                                (32 x 32 tiles through shared memory)
 //   2. t2[l][h] = sum_e VL(lo[l] + e, h) vT[l'_e][h]     (L part; FP64 partial)
 //   3. t2' = transpose(t2) into the vT buffer           (now [h][l])
-//   4. t3[r] = sum of the row's M pairs                  (CSR, LPR lanes per row; FP64 partial)
+//   4. t3[r] = sum of the row's M pairs                  (FP64 partial; see below)
 //   5. out[h][l] = t2'[h][l] + t3[r] + sum_k VH(ho[h] + k, l) v[h'_k][l]
 // Steps 2 and 5 are one kernel (k_slab) over an A x B grid of outputs (A slabs of B rows each,
 // A = nh for H, A = nl for L): a warp owns one slab a and 32 consecutive b (one "panel"), a
@@ -23,7 +23,11 @@
 // gathered vector stays in L2 while all slabs pass over it.  The elements are stored in the
 // same panel-major order, VH(k, l) at ((l / 32) * KH + k) * 32 + l % 32 (KH = entries of all
 // slabs), so the element stream of a panel pass is one contiguous sweep.  Source indices are
-// kept premultiplied (h' * nl, l' * nh).  Both slab passes are bound by the L2 -> SM traffic of
+// kept premultiplied (h' * nl, l' * nh).
+// Step 4: when all M source slabs of every slab fit in shared memory together (small slabs,
+// e.g. 512 strings per half), k_tail_smem stages them per block and gathers from shared
+// memory through 16-bit indices of a compact copy of the row tails; otherwise (and under
+// SQD_LAYOUT_PRODUCT_CSR) the CSR kernel runs over the row tails, gathering from global memory.  Both slab passes are bound by the L2 -> SM traffic of
 // the coalesced amplitude reads (one amplitude per entry, served by L2) rather than by DRAM.
 // FP32 vectors keep the compensated accumulation in every part and pass partials in FP64, so
 // the result is rounded once.  The elements are the same numbers as in the CSR arrays; only
@@ -301,6 +305,179 @@ k_mv_mixed(const int64_t* __restrict__ row_ptr, const uint32_t* __restrict__ col
   }
 }
 
+// ---- M pairs through shared memory ----------------------------------------------------
+constexpr int kTailThreads = 512;
+constexpr size_t kTailSmemMax = 200 * 1024;
+
+__device__ __forceinline__ int64_t tail_begin(const int64_t* row_ptr, const int64_t* ho,
+                                              const int64_t* lo, int64_t r, int64_t nl) {
+  const int64_t h = r / nl, l = r - h * nl;
+  return row_ptr[r] + (ho[h + 1] - ho[h]) + (lo[l + 1] - lo[l]);
+}
+
+// bits[h][h' / 32] |= 1 << (h' % 32) for every M source slab h' of slab h; per-row tail lengths.
+__global__ void k_tail_mark(const int64_t* __restrict__ row_ptr, const uint32_t* __restrict__ cols,
+                            const int64_t* __restrict__ ho, const int64_t* __restrict__ lo,
+                            int64_t n, int64_t nl, int64_t words, uint32_t* bits, int64_t* len) {
+  for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n;
+       r += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t h = r / nl;
+    const int64_t b = tail_begin(row_ptr, ho, lo, r, nl), e = row_ptr[r + 1];
+    len[r] = e - b;
+    for (int64_t i = b; i < e; ++i) {
+      const uint32_t hs = static_cast<uint32_t>(cols[i] / nl);
+      atomicOr(bits + h * words + (hs >> 5), 1u << (hs & 31));
+    }
+  }
+}
+
+__global__ void k_tail_counts(const uint32_t* __restrict__ bits, int64_t nh, int64_t words,
+                              int64_t* counts, unsigned* max_count) {
+  for (int64_t h = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; h < nh;
+       h += int64_t(gridDim.x) * blockDim.x) {
+    int64_t c = 0;
+    for (int64_t w = 0; w < words; ++w) c += __popc(bits[h * words + w]);
+    counts[h] = c;
+    atomicMax(max_count, static_cast<unsigned>(c));
+  }
+}
+
+__global__ void k_tail_slist(const uint32_t* __restrict__ bits, int64_t nh, int64_t words,
+                             const int64_t* __restrict__ soff, uint32_t* slist) {
+  for (int64_t h = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; h < nh;
+       h += int64_t(gridDim.x) * blockDim.x) {
+    int64_t k = soff[h];
+    for (int64_t w = 0; w < words; ++w) {
+      uint32_t m = bits[h * words + w];
+      while (m) {
+        const int bit = __ffs(m) - 1;
+        m &= m - 1;
+        slist[k++] = static_cast<uint32_t>(w * 32 + bit);
+      }
+    }
+  }
+}
+
+// Compact tail copy: element and shared-memory index (slot of h' among h's sources).
+template <int NCA>
+__global__ void k_tail_fill(const int64_t* __restrict__ row_ptr, const uint32_t* __restrict__ cols,
+                            const double* __restrict__ vals, const int64_t* __restrict__ ho,
+                            const int64_t* __restrict__ lo, const uint32_t* __restrict__ bits,
+                            int64_t n, int64_t nl, int64_t words,
+                            const int64_t* __restrict__ mptr, uint16_t* msidx, double* mval,
+                            int with_index) {
+  for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n;
+       r += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t h = r / nl;
+    const int64_t b = tail_begin(row_ptr, ho, lo, r, nl), e = row_ptr[r + 1];
+    int64_t j = mptr[r];
+    for (int64_t i = b; i < e; ++i, ++j) {
+#pragma unroll
+      for (int t = 0; t < NCA; ++t) mval[NCA * j + t] = vals[NCA * i + t];
+      if (!with_index) continue;
+      const int64_t c = cols[i];
+      const int64_t hs = c / nl;
+      int64_t slot = 0;
+      for (int64_t w = 0; w < (hs >> 5); ++w) slot += __popc(bits[h * words + w]);
+      slot += __popc(bits[h * words + (hs >> 5)] & ((1u << (hs & 31)) - 1u));
+      msidx[j] = static_cast<uint16_t>(slot * nl + (c - hs * nl));
+    }
+  }
+}
+
+template <typename R, int NC>
+__device__ __forceinline__ Cx<R> sm_elem(const R* p, int64_t i) {
+  if constexpr (NC == 2) {
+    if constexpr (sizeof(R) == 8) {
+      const double2 d = reinterpret_cast<const double2*>(p)[i];
+      return cx_make<R>(d.x, d.y);
+    } else {
+      const float2 d = reinterpret_cast<const float2*>(p)[i];
+      return cx_make<R>(d.x, d.y);
+    }
+  } else {
+    return cx_make<R>(p[i], R(0));
+  }
+}
+
+// M pairs of the rows of slab h (split in `chunks` row ranges, one block each): the block
+// copies all M source slabs of h into shared memory once, then LPR lanes per row stream the
+// compact tail (element + 16-bit shared-memory index) and gather from shared memory.
+template <typename R, int NCV, int NCA, int LPR>
+__global__ void __launch_bounds__(kTailThreads)
+k_tail_smem(const int64_t* __restrict__ mptr, const uint16_t* __restrict__ msidx,
+            const R* __restrict__ mval, const R* __restrict__ v, const int64_t* __restrict__ soff,
+            const uint32_t* __restrict__ slist, int64_t nh, int64_t nl, int64_t chunks,
+            double* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char tail_raw[];
+  using E = std::conditional_t<NCV == 2, std::conditional_t<sizeof(R) == 8, double2, float2>, R>;
+  E* vse = reinterpret_cast<E*>(tail_raw);
+  const R* vs = reinterpret_cast<const R*>(tail_raw);
+  const E* ve = reinterpret_cast<const E*>(v);
+  constexpr int RPW = 32 / LPR;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sub = lane % LPR, slot = lane / LPR;
+  const int nwarps = blockDim.x >> 5;
+  const int64_t per_chunk = (nl + chunks - 1) / chunks;
+  for (int64_t blk = blockIdx.x; blk < nh * chunks; blk += gridDim.x) {
+    const int64_t h = blk / chunks, c = blk - h * chunks;
+    const int64_t s0 = __ldg(soff + h), s1 = __ldg(soff + h + 1);
+    __syncthreads();  // the previous block's slabs are consumed
+    for (int64_t s = s0; s < s1; ++s) {
+      const int64_t base = int64_t(__ldg(slist + s)) * nl;
+      E* dst = vse + (s - s0) * nl;
+      for (int64_t i = threadIdx.x; i < nl; i += blockDim.x) dst[i] = ve[base + i];
+    }
+    __syncthreads();
+    const int64_t l0 = c * per_chunk, l1 = min(nl, l0 + per_chunk);
+    for (int64_t lb = l0 + int64_t(warp) * RPW; lb < l1; lb += int64_t(nwarps) * RPW) {
+      const int64_t l = lb + slot;
+      CAcc<R, NCV, NCA> acc;
+      if (l < l1) {
+        const int64_t r = h * nl + l;
+        const int64_t e = __ldg(mptr + r + 1);
+        int64_t i = __ldg(mptr + r) + sub;
+        for (; i + 3 * LPR < e; i += 4 * LPR) {
+          uint16_t si[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) si[u] = __ldg(msidx + i + u * LPR);
+          Cx<R> a[4], x[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            a[u] = ld_elem<R, NCA>(mval, i + u * LPR);
+            x[u] = sm_elem<R, NCV>(vs, si[u]);
+          }
+          acc.add4(a, x);
+        }
+        for (; i < e; i += LPR) acc.add(ld_elem<R, NCA>(mval, i), sm_elem<R, NCV>(vs, __ldg(msidx + i)));
+      }
+      acc.merge(LPR);
+      if (sub == 0 && l < l1) acc.store_partial(part, h * nl + l);
+    }
+  }
+}
+
+template <typename R, int NCV, int NCA>
+void allow_tail_smem() {
+  const int bytes = static_cast<int>(kTailSmemMax);
+  const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  SQD_CUDA(cudaFuncSetAttribute(k_tail_smem<R, NCV, NCA, 1>, attr, bytes));
+  SQD_CUDA(cudaFuncSetAttribute(k_tail_smem<R, NCV, NCA, 2>, attr, bytes));
+  SQD_CUDA(cudaFuncSetAttribute(k_tail_smem<R, NCV, NCA, 4>, attr, bytes));
+  SQD_CUDA(cudaFuncSetAttribute(k_tail_smem<R, NCV, NCA, 8>, attr, bytes));
+  SQD_CUDA(cudaFuncSetAttribute(k_tail_smem<R, NCV, NCA, 16>, attr, bytes));
+  SQD_CUDA(cudaFuncSetAttribute(k_tail_smem<R, NCV, NCA, 32>, attr, bytes));
+}
+
+void allow_tail_smem_all() {
+  allow_tail_smem<double, 1, 1>();
+  allow_tail_smem<double, 2, 1>();
+  allow_tail_smem<double, 2, 2>();
+  allow_tail_smem<float, 1, 1>();
+  allow_tail_smem<float, 2, 1>();
+  allow_tail_smem<float, 2, 2>();
+}
+
 unsigned capped_grid(int64_t blocks) {
   return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(blocks, INT_MAX)));
 }
@@ -351,6 +528,98 @@ void to_float(const DevBuf<double>& in, DevBuf<float>& out, cudaStream_t st) {
   k_to_float32<<<grid_for(static_cast<int64_t>(in.count), 256, 16384), 256, 0, st>>>(
       in.ptr, out.ptr, static_cast<int64_t>(in.count));
   SQD_CHECK_LAUNCH();
+}
+
+// Builds the shared-memory form of the M pairs when every slab's M source slabs fit in
+// kTailSmemMax together (at 8 bytes per amplitude) and 16-bit indices reach them.
+void build_tail(sqd_op_s* op, cudaStream_t st) {
+  ProductLayout& L = op->prod;
+  const int64_t nh = L.nh, nl = L.nl, n = nh * nl;
+  if (L.pairs_m <= 0 || nh > 65536) return;
+  const int64_t words = (nh + 31) / 32;
+  DevBuf<uint32_t> bits;
+  bits.alloc(static_cast<size_t>(nh * words), st);
+  SQD_CUDA(cudaMemsetAsync(bits.ptr, 0, sizeof(uint32_t) * nh * words, st));
+  DevBuf<int64_t> len, counts;
+  len.alloc(n, st);
+  counts.alloc(nh, st);
+  DevBuf<unsigned> maxc;
+  maxc.alloc(1, st);
+  SQD_CUDA(cudaMemsetAsync(maxc.ptr, 0, sizeof(unsigned), st));
+  const unsigned G = grid_for(n, 256, 16384);
+  k_tail_mark<<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, L.ho.ptr, L.lo.ptr, n, nl, words,
+                                 bits.ptr, len.ptr);
+  SQD_CHECK_LAUNCH();
+  k_tail_counts<<<grid_for(nh, 256, 4096), 256, 0, st>>>(bits.ptr, nh, words, counts.ptr,
+                                                          maxc.ptr);
+  SQD_CHECK_LAUNCH();
+  unsigned slots = 0;
+  copy_to_host(&slots, maxc.ptr, 1, st);
+  const int64_t span = static_cast<int64_t>(slots) * nl;
+  if (slots == 0 || span > 65535 || static_cast<size_t>(span) * 8 > kTailSmemMax) return;
+  L.soff.alloc(nh + 1, st);
+  exclusive_scan_i64(counts.ptr, L.soff.ptr, nh, true, st);
+  int64_t total = 0;
+  copy_to_host(&total, L.soff.ptr + nh, 1, st);
+  L.slist.alloc(std::max<int64_t>(total, 1), st);
+  k_tail_slist<<<grid_for(nh, 256, 4096), 256, 0, st>>>(bits.ptr, nh, words, L.soff.ptr,
+                                                         L.slist.ptr);
+  SQD_CHECK_LAUNCH();
+  L.mptr.alloc(n + 1, st);
+  exclusive_scan_i64(len.ptr, L.mptr.ptr, n, true, st);
+  const int nca = op->value_complex ? 2 : 1;
+  L.msidx.alloc(static_cast<size_t>(L.pairs_m), st);
+  L.mval.alloc(static_cast<size_t>(L.pairs_m) * nca, st);
+  if (nca == 2)
+    k_tail_fill<2><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, op->values.ptr, L.ho.ptr,
+                                      L.lo.ptr, bits.ptr, n, nl, words, L.mptr.ptr, L.msidx.ptr,
+                                      L.mval.ptr, 1);
+  else
+    k_tail_fill<1><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, op->values.ptr, L.ho.ptr,
+                                      L.lo.ptr, bits.ptr, n, nl, words, L.mptr.ptr, L.msidx.ptr,
+                                      L.mval.ptr, 1);
+  SQD_CHECK_LAUNCH();
+  allow_tail_smem_all();
+  SQD_CUDA(cudaStreamSynchronize(st));
+  L.tail_slots = static_cast<int>(slots);
+}
+
+// Tail elements again after a coefficient update (indices unchanged).
+void refill_tail(sqd_op_s* op, cudaStream_t st) {
+  ProductLayout& L = op->prod;
+  if (!L.tail_slots) return;
+  const int64_t n = L.nh * L.nl;
+  const unsigned G = grid_for(n, 256, 16384);
+  if (op->value_complex)
+    k_tail_fill<2><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, op->values.ptr, L.ho.ptr,
+                                      L.lo.ptr, nullptr, n, L.nl, 0, L.mptr.ptr, nullptr,
+                                      L.mval.ptr, 0);
+  else
+    k_tail_fill<1><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, op->values.ptr, L.ho.ptr,
+                                      L.lo.ptr, nullptr, n, L.nl, 0, L.mptr.ptr, nullptr,
+                                      L.mval.ptr, 0);
+  SQD_CHECK_LAUNCH();
+}
+
+template <typename R, int NCV, int NCA>
+bool launch_tail_smem(sqd_op_s* op, int prec, const R* vin, cudaStream_t st) {
+  ProductLayout& L = op->prod;
+  if (!L.tail_slots) return false;
+  const size_t bytes = static_cast<size_t>(L.tail_slots) * L.nl * NCV * sizeof(R);
+  if (bytes > kTailSmemMax) return false;
+  const R* mv;
+  if constexpr (sizeof(R) == 8) mv = L.mval.ptr;
+  else mv = L.mval32.ptr;
+  if (mv == nullptr) return false;
+  const int64_t chunks =
+      std::max<int64_t>(1, std::min<int64_t>(8, (4 * int64_t(num_sms()) + L.nh - 1) / L.nh));
+  dispatch_lpr(op->lanes_per_row[prec], [&](auto lpr_t) {
+    constexpr int LPR = decltype(lpr_t)::value;
+    k_tail_smem<R, NCV, NCA, LPR><<<capped_grid(L.nh * chunks), kTailThreads, bytes, st>>>(
+        L.mptr.ptr, L.msidx.ptr, mv, vin, L.soff.ptr, L.slist.ptr, L.nh, L.nl, chunks, L.t.ptr);
+    SQD_CHECK_LAUNCH();
+  });
+  return true;
 }
 
 }  // namespace
@@ -461,9 +730,11 @@ void op_product_build(sqd_op_s* op, cudaStream_t st) {
     throw Error(SQD_ERR_DEVICE, "stored sources do not follow the product structure (" +
                                     std::to_string(hbad) + " pairs)");
   }
+  build_tail(op, st);
   if (op->values32.ptr) {
     to_float(op->prod.vh, op->prod.vh32, st);
     to_float(op->prod.vl, op->prod.vl32, st);
+    if (op->prod.tail_slots) to_float(op->prod.mval, op->prod.mval32, st);
   }
   op->prod.built = 1;
   SQD_CUDA(cudaStreamSynchronize(st));
@@ -473,9 +744,11 @@ void op_product_build(sqd_op_s* op, cudaStream_t st) {
 void op_product_values(sqd_op_s* op, cudaStream_t st) {
   if (!op->prod.built) return;
   extract(op, st, 0, nullptr);
+  refill_tail(op, st);
   if (op->prod.vh32.ptr) {
     to_float(op->prod.vh, op->prod.vh32, st);
     to_float(op->prod.vl, op->prod.vl32, st);
+    if (op->prod.tail_slots) to_float(op->prod.mval, op->prod.mval32, st);
   }
 }
 
@@ -483,6 +756,7 @@ void op_product_values32(sqd_op_s* op, cudaStream_t st) {
   if (!op->prod.built || op->prod.vh32.ptr) return;
   to_float(op->prod.vh, op->prod.vh32, st);
   to_float(op->prod.vl, op->prod.vl32, st);
+  if (op->prod.tail_slots) to_float(op->prod.mval, op->prod.mval32, st);
 }
 
 void op_product_matvec(sqd_op_s* op, const void* v, void* out, int dtype, cudaStream_t st) {
@@ -521,13 +795,16 @@ void op_product_matvec(sqd_op_s* op, const void* v, void* out, int dtype, cudaSt
     launch_transpose<ED>(L.tt.ptr, L.vt.ptr, nl, nh, st);
     // 4. M part: t3[r]
     if (L.pairs_m > 0) {
-      dispatch_lpr(op->lanes_per_row[prec], [&](auto lpr_t) {
-        constexpr int LPR = decltype(lpr_t)::value;
-        k_mv_mixed<R, NCV, NCA, LPR><<<mixed_grid(n, LPR), 256, 0, st>>>(
-            op->row_ptr.ptr, op->cols.ptr, VC, vin, L.ho.ptr, L.lo.ptr, nl, L.t.ptr, n,
-            op->chunk_rows[prec]);
-        SQD_CHECK_LAUNCH();
-      });
+      if (op->layout[prec] == SQD_LAYOUT_PRODUCT_CSR ||
+          !launch_tail_smem<R, NCV, NCA>(op, prec, vin, st)) {
+        dispatch_lpr(op->lanes_per_row[prec], [&](auto lpr_t) {
+          constexpr int LPR = decltype(lpr_t)::value;
+          k_mv_mixed<R, NCV, NCA, LPR><<<mixed_grid(n, LPR), 256, 0, st>>>(
+              op->row_ptr.ptr, op->cols.ptr, VC, vin, L.ho.ptr, L.lo.ptr, nl, L.t.ptr, n,
+              op->chunk_rows[prec]);
+          SQD_CHECK_LAUNCH();
+        });
+      }
       // 5. H part plus both partials
       launch_slab<R, NCV, NCA, true, true>(nh, nl, L.th, L.ho.ptr, L.hsrc.ptr, VH, vin, L.vt.ptr,
                                            L.t.ptr, vout, nullptr, st);
@@ -546,8 +823,10 @@ extern "C" int sqd_op_set_layout(sqd_op_t op, int precision, int layout, void* s
   return guarded([&] {
     SQD_REQUIRE(op != nullptr, "NULL operator");
     SQD_REQUIRE(precision == 0 || precision == 1, "precision must be 0 (FP64) or 1 (FP32)");
-    SQD_REQUIRE(layout == SQD_LAYOUT_CSR || layout == SQD_LAYOUT_PRODUCT, "unknown layout");
-    if (layout == SQD_LAYOUT_PRODUCT) {
+    SQD_REQUIRE(layout == SQD_LAYOUT_CSR || layout == SQD_LAYOUT_PRODUCT ||
+                    layout == SQD_LAYOUT_PRODUCT_CSR,
+                "unknown layout");
+    if (layout != SQD_LAYOUT_CSR) {
       cudaStream_t st = as_stream(stream);
       op_product_build(op, st);
       if (precision == 1) {

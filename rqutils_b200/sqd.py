@@ -194,13 +194,14 @@ class SQDOperator:
         """precision 0: FP64 vectors (float64/complex128), 1: FP32 vectors."""
         _lib.call('sqd_op_set_lanes', self._handle, int(precision), int(lanes))
 
-    LAYOUTS = {'csr': 0, 'product': 1}
+    LAYOUTS = {'csr': 0, 'product': 1, 'product-csr': 2}
 
     def set_layout(self, precision, layout):
         """Element layout of the cached matvec for one precision: 'csr' (one pair list per
-        row) or 'product' (dense slabs for the pairs that change one half of the qubits, the
-        other pairs kept in CSR lists).  The product layout needs a product subspace and is
-        built on first use."""
+        row), 'product' (dense slabs for the pairs that change one half of the qubits; the
+        other pairs gather from shared memory when their source slabs fit there) or
+        'product-csr' (the same slabs, the other pairs always on CSR lists).  The product
+        layouts need a product subspace and are built on first use."""
         _lib.call('sqd_op_set_layout', self._handle, int(precision), self.LAYOUTS[layout],
                   _lib.stream_ptr())
 

@@ -58,18 +58,19 @@ def test_product_layout_matches_csr_and_oracle(dtype):
     csr = op.matvec(v).cpu().numpy()
     ref = _oracle_hv(wl.x, wl.z, wl.coeffs, wl.states, n, v.cpu().numpy(), True)
     tol = MATVEC_RTOL if prec == 0 else MATVEC32_RTOL
-    op.set_layout(prec, 'product')
-    assert op.get_layout(prec) == 'product' and op.get_layout(1 - prec) == 'csr'
-    info = op.product_info()
-    assert info['pairs_high'] + info['pairs_low'] + info['pairs_mixed'] == op.nnz
-    assert min(info['pairs_high'], info['pairs_low'], info['pairs_mixed']) > 0
-    for lanes in (1, 4, 32):
-        for chunk in (0, 64):
-            op.set_lanes(prec, lanes)
-            op.set_chunk(prec, chunk)
-            got = op.matvec(v).cpu().numpy()
-            assert rel(got, ref) < tol
-            assert rel(got, csr) < (MATVEC_RTOL if prec == 0 else MATVEC32_RTOL)
+    for layout in ('product', 'product-csr'):
+        op.set_layout(prec, layout)
+        assert op.get_layout(prec) == layout and op.get_layout(1 - prec) == 'csr'
+        info = op.product_info()
+        assert info['pairs_high'] + info['pairs_low'] + info['pairs_mixed'] == op.nnz
+        assert min(info['pairs_high'], info['pairs_low'], info['pairs_mixed']) > 0
+        for lanes in (1, 4, 32):
+            for chunk in (0, 64):
+                op.set_lanes(prec, lanes)
+                op.set_chunk(prec, chunk)
+                got = op.matvec(v).cpu().numpy()
+                assert rel(got, ref) < tol
+                assert rel(got, csr) < (MATVEC_RTOL if prec == 0 else MATVEC32_RTOL)
 
 
 @pytest.mark.parametrize('dtype', [torch.complex128, torch.complex64])
@@ -82,9 +83,10 @@ def test_product_layout_complex_elements(dtype):
     assert op.value_complex
     v = _vector(op.size, dtype, seed=5)
     ref = _oracle_hv(x, z, c, states, 16, v.cpu().numpy(), False)
-    op.set_layout(PREC[dtype], 'product')
-    got = op.matvec(v).cpu().numpy()
-    assert rel(got, ref) < (MATVEC_RTOL if PREC[dtype] == 0 else MATVEC32_RTOL)
+    for layout in ('product', 'product-csr'):
+        op.set_layout(PREC[dtype], layout)
+        got = op.matvec(v).cpu().numpy()
+        assert rel(got, ref) < (MATVEC_RTOL if PREC[dtype] == 0 else MATVEC32_RTOL)
 
 
 def test_product_layout_without_two_half_pairs_or_diagonal():
@@ -140,11 +142,14 @@ def test_product_layout_locg_autotune_and_refresh():
     for mode in ('fp64', 'mixed'):
         e, _, _ = rq.ground_locg(op, x0, mode=mode)
         assert abs(e - e_csr) <= 1e-10 * abs(e_csr)
-    # coefficient update: the slabs follow the refreshed elements
+    # coefficient update: the slabs and the tail copies follow the refreshed elements
     c2 = wl.coeffs * 1.3
     ham.set_coeffs(torch.as_tensor(c2))
     op.refresh()
     v = _vector(op.size, torch.complex128, seed=2)
     ref = _oracle_hv(wl.x, wl.z, c2, wl.states, n, v.cpu().numpy(), True)
-    assert rel(op.matvec(v).cpu().numpy(), ref) < MATVEC_RTOL
-    assert rel(op.matvec(v.to(torch.complex64)).cpu().numpy(), ref) < MATVEC32_RTOL
+    for layout in ('product', 'product-csr'):
+        op.set_layout(0, layout)
+        op.set_layout(1, layout)
+        assert rel(op.matvec(v).cpu().numpy(), ref) < MATVEC_RTOL
+        assert rel(op.matvec(v.to(torch.complex64)).cpu().numpy(), ref) < MATVEC32_RTOL
