@@ -45,6 +45,8 @@ def parse():
     ap.add_argument('--cache', default='1,2')
     ap.add_argument('--no-locg', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
+    ap.add_argument('--no-graph', action='store_true',
+                    help='LOCG without CUDA graphs (so a profiler sees every pass kernel)')
     ap.add_argument('--cpu-rows', type=int, default=0, help='CPU sample rows (0 = auto)')
     ap.add_argument('--lanes', type=int, default=0, help='lanes per row (0 = autotune)')
     ap.add_argument('--chunk', type=int, default=0, help='rows per block chunk with --lanes')
@@ -81,10 +83,13 @@ def load_peaks():
 
 def load_traffic(workload, cache, layout='csr'):
     """DRAM traffic of one matvec (all its kernels) from the committed ncu summary."""
-    suffix = '' if layout == 'csr' else f'_{layout}'
-    path = os.path.join(ROOT, 'profiles', f'matvec_{workload}_cache{cache[0]}{cache[1]}{suffix}.md')
-    if not os.path.exists(path):
+    names = [''] if layout == 'csr' else [f'_{layout}', '_product', '_product-csr']
+    paths = [os.path.join(ROOT, 'profiles', f'matvec_{workload}_cache{cache[0]}{cache[1]}{n}.md')
+             for n in names]
+    paths = [p for p in paths if os.path.exists(p)]
+    if not paths:
         return None
+    path = paths[0]
     for line in open(path):
         if line.startswith('traffic_bytes_per_launch:'):
             return float(line.split(':', 1)[1])
@@ -332,7 +337,7 @@ def run_ours(args):
 
     extra = {}
     if not args.no_locg and rank == 0:
-        extra['locg'] = locg_times(rq, op, wl, dev)
+        extra['locg'] = locg_times(rq, op, wl, dev, use_graph=not args.no_graph)
     if args.workload == 'c5' and rank == 0:
         extra['gradient'] = gradient_check(rq, op, wl)
     line = None
@@ -455,21 +460,22 @@ def gradient_check(rq, op, wl, n_coords=32, h=1e-5):
             'median_rel_err_vs_fd': float(np.median(errs))}
 
 
-def locg_times(rq, op, wl, dev):
+def locg_times(rq, op, wl, dev, use_graph=True):
     """Time-to-E0 of the FP64 path (reference algorithm) and of the mixed-precision path."""
     import torch
     x0 = torch.as_tensor(wl.start_vector(np.complex128), device=dev)
     # tol=None: the reference default (dtype epsilon in its N-scaled test, ground_locg.py:
     # 224-225, 371-376), i.e. a converged FP64 energy to compare the mixed path against.
     res = {'start_vector': 'complex128 N(0,1)+iN(0,1), normalised', 'tol': None,
-           'timing': 'median of 3 solves per mode after one short warm-up solve'}
+           'timing': 'median of 3 solves per mode after one short warm-up solve',
+           'cuda_graphs': use_graph}
     for mode in ('fp64', 'mixed'):
-        rq.ground_locg(op, x0, maxiter=3, mode=mode)   # warm-up
+        rq.ground_locg(op, x0, maxiter=3, mode=mode, use_graph=use_graph)   # warm-up
         runs = []
         for _ in range(3):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            e, vec, it = rq.ground_locg(op, x0, mode=mode)
+            e, vec, it = rq.ground_locg(op, x0, mode=mode, use_graph=use_graph)
             torch.cuda.synchronize()
             runs.append(time.perf_counter() - t0)
         res[mode] = {'time_to_e0_s': statistics.median(runs), 'runs_s': runs, 'eigval': e,
