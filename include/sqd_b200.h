@@ -41,8 +41,17 @@ enum sqd_dtype { SQD_F64 = 0, SQD_C128 = 1, SQD_F32 = 2, SQD_C64 = 3 };
 /* Flags for sqd_paulis_create. */
 #define SQD_PAULIS_FORCE_REAL 1u
 
-/* Lookup methods for the b XOR x search. */
-enum sqd_lookup { SQD_LOOKUP_HASH = 0, SQD_LOOKUP_BSEARCH = 1 };
+/* Lookup methods for the b XOR x search.  SQD_LOOKUP_PRODUCT (operators only): when the
+ * subspace is the product of strings on the high and the low half of the qubits, each half is
+ * looked up in its own sorted string list, once per string instead of once per row, and the
+ * rows' pairs are assembled from those lists (same pairs, same order); SQD_ERR_UNSUPPORTED for
+ * other subspaces.  SQD_LOOKUP_AUTO: SQD_LOOKUP_PRODUCT where it applies, else SQD_LOOKUP_HASH. */
+enum sqd_lookup {
+  SQD_LOOKUP_HASH = 0,
+  SQD_LOOKUP_BSEARCH = 1,
+  SQD_LOOKUP_AUTO = 2,
+  SQD_LOOKUP_PRODUCT = 3
+};
 
 typedef struct sqd_paulis_s* sqd_paulis_t;
 typedef struct sqd_space_s* sqd_space_t;

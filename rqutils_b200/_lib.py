@@ -15,7 +15,7 @@ SQD_OK = 0
 SQD_ERR_INVALID = -1
 SQD_F64, SQD_C128, SQD_F32, SQD_C64 = 0, 1, 2, 3
 SQD_PAULIS_FORCE_REAL = 1
-SQD_LOOKUP_HASH, SQD_LOOKUP_BSEARCH = 0, 1
+SQD_LOOKUP_HASH, SQD_LOOKUP_BSEARCH, SQD_LOOKUP_AUTO, SQD_LOOKUP_PRODUCT = 0, 1, 2, 3
 SQD_LOCG_FP64, SQD_LOCG_MIXED = 0, 1
 
 _c = ctypes

@@ -116,6 +116,8 @@ struct sqd_op_s {
   sqd::DevBuf<float> values32;    // FP32 copy for the mixed-precision matvec
   sqd::DevBuf<GroupPre> gpre;     // groups that can connect (x != 0, even sector counts)
   int64_t n_gpre = 0;
+  int64_t n_gpre_cls[3] = {0, 0, 0};  // gpre entries per class (H, L, M), in that order
+  int product_built = 0;          // connectivity assembled from the two halves' lists
   sqd::DevBuf<int> status;        // device status word
   int layout[2] = {0, 0};         // SQD_LAYOUT_* per precision
   ProductLayout prod;
@@ -166,5 +168,8 @@ void op_product_build(sqd_op_s* op, cudaStream_t st);
 void op_product_values(sqd_op_s* op, cudaStream_t st);
 void op_product_values32(sqd_op_s* op, cudaStream_t st);
 void op_product_matvec(sqd_op_s* op, const void* v, void* out, int dtype, cudaStream_t st);
+// Connectivity (row_ptr, cols, grps, nnz) of a product subspace from per-half partner lists;
+// false when the subspace is not such a product.
+bool op_connect_product(sqd_op_s* op, cudaStream_t st);
 
 }  // namespace sqd

@@ -213,7 +213,7 @@ void op_matvec(sqd_op_s* op, const void* v, void* out, int dtype, cudaStream_t s
     P.hkeys = sp->hkeys.ptr;
     P.hvals = sp->hvals.ptr;
     P.hmask = sp->hmask;
-    P.lookup = op->lookup;
+    P.lookup = op->lookup == SQD_LOOKUP_BSEARCH ? SQD_LOOKUP_BSEARCH : SQD_LOOKUP_HASH;
     P.nsec = sp->num_sectors;
     P.m0 = sp->sector_mask[0];
     P.m1 = sp->sector_mask[1];

@@ -324,12 +324,13 @@ __global__ void k_grad_offdiag(const int64_t* row_ptr, const uint32_t* cols,
 }  // namespace
 
 // ---------------------------------------------------------------------------------------------
+void op_connect_sweep(sqd_op_s* op, cudaStream_t st);
+void op_values_and_lanes(sqd_op_s* op, cudaStream_t st);
+
 void op_build(sqd_op_s* op, cudaStream_t st) {
   sqd_paulis_s* p = op->p;
   sqd_space_s* sp = op->s;
   const int64_t J = p->num_groups;
-  const int64_t size = sp->states_size;
-  const int64_t nu = sp->n_unique;
   uint64_t x0 = 1;
   copy_to_host(&x0, p->group_x.ptr, 1, st);
   op->has_diag_group = (x0 == 0) ? 1 : 0;
@@ -356,6 +357,7 @@ void op_build(sqd_op_s* op, cudaStream_t st) {
       copy_to_host(&n_cls[c], pos[c].ptr + J, 1, st);
     }
     op->n_gpre = n_cls[0] + n_cls[1] + n_cls[2];
+    for (int c = 0; c < 3; ++c) op->n_gpre_cls[c] = n_cls[c];
     op->gpre.alloc(op->n_gpre > 0 ? op->n_gpre : 1, st);
     k_gpre_fill<<<G, 256, 0, st>>>(p->group_x.ptr, J, flags[0].ptr, pos[0].ptr, flags[1].ptr,
                                   pos[1].ptr, flags[2].ptr, pos[2].ptr, sp->sector_mask[0],
@@ -364,6 +366,23 @@ void op_build(sqd_op_s* op, cudaStream_t st) {
   }
   if (op->x_cache == 0) return;
 
+  bool connected = false;
+  if (op->lookup == SQD_LOOKUP_AUTO || op->lookup == SQD_LOOKUP_PRODUCT) {
+    connected = op_connect_product(op, st);
+    if (!connected && op->lookup == SQD_LOOKUP_PRODUCT)
+      throw Error(SQD_ERR_UNSUPPORTED,
+                  "SQD_LOOKUP_PRODUCT needs a product of high-half and low-half strings without "
+                  "fill-in slots");
+  }
+  if (!connected) op_connect_sweep(op, st);
+  op_values_and_lanes(op, st);
+}
+
+// Connectivity by the (row, group) sweep: any subspace, fill-in slots included.
+void op_connect_sweep(sqd_op_s* op, cudaStream_t st) {
+  sqd_space_s* sp = op->s;
+  const int64_t size = sp->states_size;
+  const int64_t nu = sp->n_unique;
   SweepParams P{};
   P.states = sp->states.ptr;
   P.n_unique = nu;
@@ -372,7 +391,7 @@ void op_build(sqd_op_s* op, cudaStream_t st) {
   P.hkeys = sp->hkeys.ptr;
   P.hvals = sp->hvals.ptr;
   P.hmask = sp->hmask;
-  P.lookup = op->lookup;
+  P.lookup = op->lookup == SQD_LOOKUP_BSEARCH ? SQD_LOOKUP_BSEARCH : SQD_LOOKUP_HASH;
   P.nsec = sp->num_sectors;
   P.m0 = sp->sector_mask[0];
   P.m1 = sp->sector_mask[1];
@@ -423,7 +442,14 @@ void op_build(sqd_op_s* op, cudaStream_t st) {
     kern<<<tiles, SW_THREADS, dyn, st>>>(P);
     SQD_CHECK_LAUNCH();
   }
+}
 
+// Matrix elements of the stored pairs (z = 2) and the initial lanes-per-row choice.
+void op_values_and_lanes(sqd_op_s* op, cudaStream_t st) {
+  sqd_paulis_s* p = op->p;
+  sqd_space_s* sp = op->s;
+  const int64_t size = sp->states_size;
+  const int64_t nu = sp->n_unique;
   if (op->z_cache == 2) {
     const int nca = op->value_complex ? 2 : 1;
     op->values.alloc(static_cast<size_t>(op->nnz > 0 ? op->nnz : 1) * nca, st);
@@ -470,7 +496,7 @@ extern "C" int sqd_op_create(sqd_paulis_t p, sqd_space_t s, int x_cache, int z_c
                 "Pauli strings and states have different numbers of qubits");
     SQD_REQUIRE(x_cache == 0 || x_cache == 1, "x cache strategy must be 0 or 1");
     SQD_REQUIRE(z_cache >= 0 && z_cache <= 2, "z cache strategy must be 0, 1 or 2");
-    SQD_REQUIRE(lookup == SQD_LOOKUP_HASH || lookup == SQD_LOOKUP_BSEARCH, "bad lookup method");
+    SQD_REQUIRE(lookup >= SQD_LOOKUP_HASH && lookup <= SQD_LOOKUP_PRODUCT, "bad lookup method");
     auto op = std::make_unique<sqd_op_s>();
     op->p = p;
     op->s = s;

@@ -35,6 +35,7 @@
 #include <algorithm>
 #include <climits>
 #include <type_traits>
+#include <vector>
 
 #include "internal.cuh"
 #include "dispatch.cuh"
@@ -622,6 +623,157 @@ bool launch_tail_smem(sqd_op_s* op, int prec, const R* vin, cudaStream_t st) {
   return true;
 }
 
+// ---- connectivity of a product subspace -------------------------------------------------
+// The (row, group) sweep tests every group against every row.  In a product subspace a group
+// acting on one half connects a row iff the row's string of that half has a partner, so the
+// partners are searched once per string of the half, and a two-half group connects (h, l) iff
+// both halves have partners.  The pairs are then assembled per row in the sweep's order:
+// diagonal, H groups, L groups, M groups, each class in ascending group index (= ascending x:
+// for M groups, ascending high part, then low part).
+
+__device__ __forceinline__ int64_t sorted_find(const uint64_t* __restrict__ a, int64_t n,
+                                               uint64_t key) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (__ldg(a + mid) < key) lo = mid + 1; else hi = mid;
+  }
+  return (lo < n && __ldg(a + lo) == key) ? lo : -1;
+}
+
+// Partners of every string s of one half under the masks xs[k]: entries (k, partner) with
+// strs[partner] == strs[s] ^ xs[k], in k order.  One warp per string, lanes over k, ballots
+// keep the order.  COUNT: count[s]; FILL: writes at off[s].
+template <bool FILL>
+__global__ void k_half_partners(const uint64_t* __restrict__ strs, int64_t nstr,
+                                const uint64_t* __restrict__ xs, int64_t nx,
+                                const int64_t* __restrict__ off, int64_t* count,
+                                uint32_t* out_k, uint32_t* out_p) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  const int64_t w0 = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t s = w0; s < nstr; s += nw) {
+    const uint64_t base = __ldg(strs + s);
+    int64_t pos = FILL ? off[s] : 0;
+    for (int64_t k0 = 0; k0 < nx; k0 += 32) {
+      const int64_t k = k0 + lane;
+      int64_t found = -1;
+      if (k < nx) found = sorted_find(strs, nstr, base ^ __ldg(xs + k));
+      const unsigned b = __ballot_sync(kFullMask, found >= 0);
+      if (FILL && found >= 0) {
+        const int64_t idx = pos + __popc(b & lt);
+        out_k[idx] = static_cast<uint32_t>(k);
+        out_p[idx] = static_cast<uint32_t>(found);
+      }
+      pos += __popc(b);
+    }
+    if (!FILL && lane == 0) count[s] = pos;
+  }
+}
+
+struct ProdConnect {
+  int64_t nh, nl;
+  int d;
+  const int64_t *hoff, *loff, *aoff, *boff;          // H, L, M-high, M-low lists per string
+  const uint32_t *hk, *hp, *lk, *lp, *ak, *ap, *bk, *bp;
+  const int32_t *gh, *gl;                            // group index of H / L list entry k
+  const int32_t* table;                              // [na * nb] M group or -1 (dense form)
+  int64_t na, nb;
+  const uint64_t *xa, *xb, *xm;                      // sparse form: M masks, sorted
+  const int32_t* gm;
+  int64_t nm;
+};
+
+__device__ __forceinline__ int32_t m_group(const ProdConnect& c, uint32_t a, uint32_t b) {
+  if (c.table) return __ldg(c.table + int64_t(a) * c.nb + b);
+  const int64_t i = sorted_find(c.xm, c.nm, __ldg(c.xa + a) | __ldg(c.xb + b));
+  return i >= 0 ? __ldg(c.gm + i) : -1;
+}
+
+template <bool FILL>
+__global__ void k_prod_rows(ProdConnect c, int64_t* counts, const int64_t* __restrict__ row_ptr,
+                            uint32_t* cols, uint32_t* grps) {
+  const int64_t n = c.nh * c.nl;
+  for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n;
+       r += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t h = r / c.nl, l = r - h * c.nl;
+    const int64_t h0 = c.hoff[h], h1 = c.hoff[h + 1], l0 = c.loff[l], l1 = c.loff[l + 1];
+    const int64_t a0 = c.aoff[h], a1 = c.aoff[h + 1], b0 = c.boff[l], b1 = c.boff[l + 1];
+    if (!FILL) {
+      int64_t m = 0;
+      for (int64_t i = a0; i < a1; ++i)
+        for (int64_t j = b0; j < b1; ++j) m += m_group(c, c.ak[i], c.bk[j]) >= 0;
+      counts[r] = c.d + (h1 - h0) + (l1 - l0) + m;
+      continue;
+    }
+    int64_t p = row_ptr[r];
+    if (c.d) {
+      cols[p] = static_cast<uint32_t>(r);
+      grps[p] = 0;
+      ++p;
+    }
+    for (int64_t i = h0; i < h1; ++i, ++p) {
+      cols[p] = static_cast<uint32_t>(int64_t(c.hp[i]) * c.nl + l);
+      grps[p] = static_cast<uint32_t>(c.gh[c.hk[i]]);
+    }
+    for (int64_t i = l0; i < l1; ++i, ++p) {
+      cols[p] = static_cast<uint32_t>(h * c.nl + c.lp[i]);
+      grps[p] = static_cast<uint32_t>(c.gl[c.lk[i]]);
+    }
+    for (int64_t i = a0; i < a1; ++i) {
+      const int64_t src_h = int64_t(c.ap[i]) * c.nl;
+      for (int64_t j = b0; j < b1; ++j) {
+        const int32_t g = m_group(c, c.ak[i], c.bk[j]);
+        if (g < 0) continue;
+        cols[p] = static_cast<uint32_t>(src_h + c.bp[j]);
+        grps[p] = static_cast<uint32_t>(g);
+        ++p;
+      }
+    }
+  }
+}
+
+__global__ void k_half_strings(const uint64_t* __restrict__ s, int64_t count, int64_t stride,
+                               uint64_t mask, uint64_t* out) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < count;
+       i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = s[i * stride] & mask;
+}
+
+// Device copy of a host vector.
+template <typename T>
+void upload(DevBuf<T>& d, const std::vector<T>& h, cudaStream_t st) {
+  d.alloc(std::max<size_t>(h.size(), 1), st);
+  if (!h.empty())
+    SQD_CUDA(cudaMemcpyAsync(d.ptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+// Partner lists of one half: counts, offsets, (k, partner) entries.
+struct HalfLists {
+  DevBuf<int64_t> off;
+  DevBuf<uint32_t> k, p;
+};
+
+void half_lists(const DevBuf<uint64_t>& strs, int64_t nstr, const DevBuf<uint64_t>& xs,
+                int64_t nx, HalfLists& out, cudaStream_t st) {
+  DevBuf<int64_t> cnt;
+  cnt.alloc(std::max<int64_t>(nstr, 1), st);
+  const unsigned G = grid_for(nstr * 32, 256, 8192);
+  k_half_partners<false><<<G, 256, 0, st>>>(strs.ptr, nstr, xs.ptr, nx, nullptr, cnt.ptr,
+                                             nullptr, nullptr);
+  SQD_CHECK_LAUNCH();
+  out.off.alloc(nstr + 1, st);
+  exclusive_scan_i64(cnt.ptr, out.off.ptr, nstr, true, st);
+  int64_t total = 0;
+  copy_to_host(&total, out.off.ptr + nstr, 1, st);
+  out.k.alloc(std::max<int64_t>(total, 1), st);
+  out.p.alloc(std::max<int64_t>(total, 1), st);
+  k_half_partners<true><<<G, 256, 0, st>>>(strs.ptr, nstr, xs.ptr, nx, out.off.ptr, nullptr,
+                                            out.k.ptr, out.p.ptr);
+  SQD_CHECK_LAUNCH();
+}
+
 }  // namespace
 
 bool op_product_detect(sqd_op_s* op, cudaStream_t st, int64_t* nh_out, int64_t* nl_out) {
@@ -647,6 +799,107 @@ bool op_product_detect(sqd_op_s* op, cudaStream_t st, int64_t* nh_out, int64_t* 
   if (bad) return false;
   *nh_out = static_cast<int64_t>(nh);
   *nl_out = nl;
+  return true;
+}
+
+bool op_connect_product(sqd_op_s* op, cudaStream_t st) {
+  int64_t nh = 0, nl = 0;
+  if (!op_product_detect(op, st, &nh, &nl)) return false;
+  sqd_space_s* sp = op->s;
+  const int64_t n = nh * nl;
+  if (n > (int64_t(1) << 32)) return false;
+  const uint64_t mlo = half_mask_low(sp->num_qubits), mhi = sp->fill_state & ~mlo;
+  // Group lists per class from the preprocessed groups (class order, ascending group index).
+  std::vector<GroupPre> gp(static_cast<size_t>(op->n_gpre));
+  copy_to_host(gp.data(), op->gpre.ptr, gp.size(), st);
+  const int64_t n0 = op->n_gpre_cls[0], n1 = op->n_gpre_cls[1];
+  std::vector<uint64_t> xh, xl, xm;
+  std::vector<int32_t> gh, gl, gm;
+  for (int64_t i = 0; i < op->n_gpre; ++i) {
+    const GroupPre& g = gp[static_cast<size_t>(i)];
+    if (i < n0) { xh.push_back(g.x); gh.push_back(g.group); }
+    else if (i < n0 + n1) { xl.push_back(g.x); gl.push_back(g.group); }
+    else { xm.push_back(g.x); gm.push_back(g.group); }
+  }
+  // Distinct high and low parts of the M masks (ascending), and the M group lookup.
+  std::vector<uint64_t> xa, xb;
+  for (uint64_t x : xm) { xa.push_back(x & mhi); xb.push_back(x & mlo); }
+  std::sort(xa.begin(), xa.end());
+  xa.erase(std::unique(xa.begin(), xa.end()), xa.end());
+  std::sort(xb.begin(), xb.end());
+  xb.erase(std::unique(xb.begin(), xb.end()), xb.end());
+  const bool dense = !xm.empty() && double(xa.size()) * double(xb.size()) <= double(1 << 24);
+  std::vector<int32_t> table;
+  if (dense) {
+    table.assign(xa.size() * xb.size(), -1);
+    for (size_t i = 0; i < xm.size(); ++i) {
+      const size_t a = std::lower_bound(xa.begin(), xa.end(), xm[i] & mhi) - xa.begin();
+      const size_t b = std::lower_bound(xb.begin(), xb.end(), xm[i] & mlo) - xb.begin();
+      table[a * xb.size() + b] = gm[i];
+    }
+  }
+  DevBuf<uint64_t> hstr, lstr, dxh, dxl, dxa, dxb, dxm;
+  DevBuf<int32_t> dgh, dgl, dgm, dtable;
+  hstr.alloc(nh, st);
+  lstr.alloc(nl, st);
+  k_half_strings<<<grid_for(nh, 256, 4096), 256, 0, st>>>(sp->states.ptr, nh, nl, mhi, hstr.ptr);
+  k_half_strings<<<grid_for(nl, 256, 4096), 256, 0, st>>>(sp->states.ptr, nl, 1, mlo, lstr.ptr);
+  SQD_CHECK_LAUNCH();
+  upload(dxh, xh, st);
+  upload(dxl, xl, st);
+  upload(dxa, xa, st);
+  upload(dxb, xb, st);
+  upload(dxm, xm, st);
+  upload(dgh, gh, st);
+  upload(dgl, gl, st);
+  upload(dgm, gm, st);
+  if (dense) upload(dtable, table, st);
+  HalfLists H, Lh, A, Bl;
+  half_lists(hstr, nh, dxh, static_cast<int64_t>(xh.size()), H, st);
+  half_lists(lstr, nl, dxl, static_cast<int64_t>(xl.size()), Lh, st);
+  half_lists(hstr, nh, dxa, static_cast<int64_t>(xa.size()), A, st);
+  half_lists(lstr, nl, dxb, static_cast<int64_t>(xb.size()), Bl, st);
+  ProdConnect c{};
+  c.nh = nh;
+  c.nl = nl;
+  c.d = op->has_diag_group;
+  c.hoff = H.off.ptr;
+  c.loff = Lh.off.ptr;
+  c.aoff = A.off.ptr;
+  c.boff = Bl.off.ptr;
+  c.hk = H.k.ptr;
+  c.hp = H.p.ptr;
+  c.lk = Lh.k.ptr;
+  c.lp = Lh.p.ptr;
+  c.ak = A.k.ptr;
+  c.ap = A.p.ptr;
+  c.bk = Bl.k.ptr;
+  c.bp = Bl.p.ptr;
+  c.gh = dgh.ptr;
+  c.gl = dgl.ptr;
+  c.table = dense ? dtable.ptr : nullptr;
+  c.na = static_cast<int64_t>(xa.size());
+  c.nb = static_cast<int64_t>(xb.size());
+  c.xa = dxa.ptr;
+  c.xb = dxb.ptr;
+  c.xm = dxm.ptr;
+  c.gm = dgm.ptr;
+  c.nm = static_cast<int64_t>(xm.size());
+  DevBuf<int64_t> counts;
+  counts.alloc(n, st);
+  const unsigned G = grid_for(n, 256, 16384);
+  k_prod_rows<false><<<G, 256, 0, st>>>(c, counts.ptr, nullptr, nullptr, nullptr);
+  SQD_CHECK_LAUNCH();
+  op->row_ptr.alloc(n + 1, st);
+  exclusive_scan_i64(counts.ptr, op->row_ptr.ptr, n, true, st);
+  copy_to_host(&op->nnz, op->row_ptr.ptr + n, 1, st);
+  counts.release();
+  op->cols.alloc(op->nnz > 0 ? op->nnz : 1, st);
+  op->grps.alloc(op->nnz > 0 ? op->nnz : 1, st);
+  k_prod_rows<true><<<G, 256, 0, st>>>(c, nullptr, op->row_ptr.ptr, op->cols.ptr, op->grps.ptr);
+  SQD_CHECK_LAUNCH();
+  SQD_CUDA(cudaStreamSynchronize(st));  // the host vectors above go out of scope
+  op->product_built = 1;
   return true;
 }
 

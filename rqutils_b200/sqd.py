@@ -32,7 +32,8 @@ from .ground_locg import ground_locg
 
 LOG = logging.getLogger(__name__)
 
-_LOOKUPS = {'hash': _lib.SQD_LOOKUP_HASH, 'bsearch': _lib.SQD_LOOKUP_BSEARCH}
+_LOOKUPS = {'hash': _lib.SQD_LOOKUP_HASH, 'bsearch': _lib.SQD_LOOKUP_BSEARCH,
+            'auto': _lib.SQD_LOOKUP_AUTO, 'product': _lib.SQD_LOOKUP_PRODUCT}
 
 
 @dataclass(frozen=True)
@@ -44,7 +45,7 @@ class SQDOptions:
     locg_maxiter: int = 1000
     locg_tol: float | None = None
     # --- extensions
-    lookup: str = 'hash'             # 'hash' or 'bsearch' for the b XOR x search
+    lookup: str = 'auto'             # b XOR x search: 'hash', 'bsearch', 'product' or 'auto'
     locg_mode: str = 'fp64'          # 'fp64' (reference algorithm) or 'mixed'
     use_graph: bool = True           # run the LOCG loop as one CUDA graph
     lanes_per_row: Optional[int] = None   # matvec schedule; None = from the mean row length
@@ -131,7 +132,7 @@ class Subspace:
 class SQDOperator:
     """The Hamiltonian projected on a subspace; callable as ``op(v) -> Hv``."""
 
-    def __init__(self, hamiltonian, space, cache_strategy=(1, 0), lookup='hash',
+    def __init__(self, hamiltonian, space, cache_strategy=(1, 0), lookup='auto',
                  lanes_per_row=None):
         self.hamiltonian = hamiltonian
         self.space = space

@@ -153,3 +153,46 @@ def test_product_layout_locg_autotune_and_refresh():
         op.set_layout(1, layout)
         assert rel(op.matvec(v).cpu().numpy(), ref) < MATVEC_RTOL
         assert rel(op.matvec(v.to(torch.complex64)).cpu().numpy(), ref) < MATVEC32_RTOL
+
+
+def _connectivity_cases():
+    wl = _jw_small(3)
+    yield wl.x, wl.z, wl.coeffs, wl.states, True
+    rng = np.random.default_rng(21)
+    x, z, c = W.random_pauli_sum(16, 400, rng, wmax=4)
+    yield x, z, c, W.product_subspace(8, 4, 27, 31, rng), False
+    xl, zl, cl = W.random_pauli_sum(8, 50, rng, wmin=1, wmax=3)
+    keep = xl != 0                                   # no Z-only terms: no diagonal group
+    yield (np.concatenate([xl[keep], xl[keep] << np.uint64(8)]),
+           np.concatenate([zl[keep], zl[keep] << np.uint64(8)]),
+           np.concatenate([cl[keep], cl[keep]]), W.product_subspace(8, 4, 19, 23, rng), True)
+
+
+@pytest.mark.parametrize('case', range(3))
+def test_product_connectivity_equals_sweep(case):
+    """Pairs assembled from per-half partner lists: the same CSR (row pointers, sources,
+    elements, order) as the (row, group) sweep, bit for bit."""
+    x, z, c, states, real = list(_connectivity_cases())[case]
+    ham = rq.PauliSumXZ.from_xz(x, z, c, 16, force_real=real, padded=True)
+    space = rq.Subspace.from_u64(states, 16)
+    sweep = rq.SQDOperator(ham, space, cache_strategy=(1, 2), lookup='hash')
+    prod = rq.SQDOperator(ham, space, cache_strategy=(1, 2), lookup='product')
+    auto = rq.SQDOperator(ham, space, cache_strategy=(1, 2), lookup='auto')
+    assert sweep.nnz == prod.nnz == auto.nnz
+    a, b = sweep.csr(), prod.csr()
+    for u, w in zip(a, b):
+        np.testing.assert_array_equal(u.cpu().numpy(), w.cpu().numpy())
+    v = _vector(sweep.size, torch.complex128, seed=case)
+    torch.testing.assert_close(prod.matvec(v), sweep.matvec(v), rtol=0, atol=0)
+
+
+def test_product_lookup_needs_a_product_subspace():
+    wl = W.c1(0)
+    ham = rq.PauliSumXZ.from_xz(wl.x, wl.z, wl.coeffs, 16, force_real=True, padded=True)
+    space = rq.Subspace.from_u64(wl.states, 16)
+    with pytest.raises(SQDError):
+        rq.SQDOperator(ham, space, cache_strategy=(1, 2), lookup='product')
+    auto = rq.SQDOperator(ham, space, cache_strategy=(1, 2), lookup='auto')   # sweep fallback
+    ref = rq.SQDOperator(ham, space, cache_strategy=(1, 2), lookup='hash')
+    v = _vector(ref.size, torch.complex128)
+    torch.testing.assert_close(auto.matvec(v), ref.matvec(v), rtol=0, atol=0)
