@@ -41,7 +41,7 @@ def parse():
     ap.add_argument('--steps', type=int, default=20)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--workload', default='c2', choices=['c1', 'c2', 'c3', 'c4', 'c5'])
+    ap.add_argument('--workload', default='c2', choices=['c1', 'c2', 'c3', 'c4', 'c5', 'c3_small'])
     ap.add_argument('--cache', default='1,2')
     ap.add_argument('--no-locg', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
@@ -57,13 +57,13 @@ def parse():
 
 def make_workload(name):
     from rqutils_b200 import workloads as W
-    return {'c1': W.c1, 'c2': W.c2, 'c3': W.c3, 'c5': W.c5}[name](0)
+    return {'c1': W.c1, 'c2': W.c2, 'c3': W.c3, 'c5': W.c5, 'c3_small': W.c3_small}[name](0)
 
 
 def workload_config(wl, cache):
     cfg = {'workload': f'{wl.name}: {wl.num_qubits}-qubit '
                        + ('JW molecular Hamiltonian, alpha x beta product subspace'
-                          if wl.name in ('c2', 'c3') else 'random Pauli sum, weight subspace'),
+                          if wl.name in ('c2', 'c3', 'c3_small') else 'random Pauli sum, weight subspace'),
            'num_qubits': wl.num_qubits, 'subspace_dim': int(wl.states.shape[0]),
            'raw_terms': int(wl.coeffs.shape[0]), 'seed': wl.seed,
            'cache_strategy': list(cache), 'vector_dtype': 'complex128',

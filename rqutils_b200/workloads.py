@@ -392,6 +392,12 @@ def c3(seed=0):
     return jw_workload('c3', 24, 6, 4096, 4096, seed)
 
 
+def c3_small(seed=0, na=1536, nb=1536):
+    """c3's Hamiltonian construction on a 1536 x 1536 product subspace (D = 2,359,296): the
+    same orbital count and pair classes at a size that full profiler captures allow."""
+    return jw_workload('c3_small', 24, 6, na, nb, seed)
+
+
 def c4_dims(seed=0, count=96):
     rng = np.random.default_rng(seed)
     lo, hi = math.log(64), math.log(1820)
