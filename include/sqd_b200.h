@@ -205,7 +205,9 @@ enum sqd_locg_mode {
  *  n, dtype: vector space (SQD_F64 or SQD_C128 for the result).
  *  fn/ctx: the operator; for SQD_LOCG_MIXED ctx must be an sqd_op_t and fn sqd_op_matvec_cb.
  *  xinit: start vector (device, dtype) or NULL for the one-hot vector at xinit_index.
- *  orth/n_orth: device vectors to orthogonalize against (ground_locg `orth`), n_orth <= 8.
+ *  orth/n_orth: device vectors to orthogonalize against (ground_locg `orth`), n_orth <= 8;
+ *  in SQD_LOCG_MIXED the FP32 sweeps project every search direction against FP32 copies
+ *  and the FP64 refinement runs the reference iteration with the vectors themselves.
  *  tol < 0 selects the dtype epsilon (:224-225).
  *  use_graph: capture each iteration in a CUDA graph (only with fn == sqd_op_matvec_cb).
  *  Outputs: eigval_host, eigvec (device, n elements of dtype), niter_host, and

@@ -907,7 +907,7 @@ class Locg {
   // Same Rayleigh-Ritz recurrence, but A x and A y are carried along as the same linear
   // combinations as x and y, so an iteration needs one matvec (A p).  Used for the FP32
   // sweeps of the mixed-precision solver; refresh() recomputes A x and A y to cancel drift.
-  void start_implicit() {
+  void start_implicit(const std::vector<const void*>& orth = {}) {
     R* x = x_.ptr;
     lc({x}, {}, {{0, 0}}, P_INV_NORM);
     lc({x}, {x}, {}, P_NONE);
@@ -921,6 +921,7 @@ class Locg {
       return;
     }
     lc({r_.ptr}, {p_.ptr}, {}, P_NONE);
+    project_orth(orth, p_.ptr, false, G_NONE);
     matvec(p_.ptr, ap_.ptr);
     lc({x, p_.ptr, ax_.ptr, ap_.ptr}, {}, {{0, 2}, {1, 2}, {1, 3}}, P_RR2);
     lc({ax_.ptr, ap_.ptr}, {ay_.ptr, ax_.ptr}, {}, P_NONE);          // A t, A u
@@ -938,12 +939,15 @@ class Locg {
   // the Gram matrix of {x, y, p} comes from the carried A x, A y and the new A p, and
   // x, y, A x, A y, r and the next step's first projection coefficients are produced in two
   // passes.
-  void body_fast() {
+  void body_fast(const std::vector<const void*>& orth) {
     R *x = x_.ptr, *y = y_.ptr, *r = r_.ptr, *p = p_.ptr;
     R *ax = ax_.ptr, *ay = ay_.ptr, *ap = ap_.ptr;
     const int g = G_DONE;
     lc({r, x, y}, {p}, {{100, 100}, {1, 100}, {2, 100}}, P_PROJ_NORM_IPS, g);
     lc({p, x, y}, {p}, {}, P_NONE, g);
+    // Orthogonality constraints (excited states): the search direction leaves their span;
+    // the Gram pass measures |p| afresh.
+    project_orth(orth, p, false, g);
     matvec(p, ap);
     lc({x, y, p, ax, ay, ap}, {},
        {{0, 3}, {1, 4}, {2, 5}, {1, 3}, {2, 3}, {2, 4}, {2, 2}, {1, 2}}, P_GRAM_IMPLICIT, g);
@@ -980,7 +984,7 @@ class Locg {
     read_host();
     if (maxiter <= 0 || host_->done) return;
     auto run_body = [&] {
-      if (fast) body_fast();
+      if (fast) body_fast(orth);
       else body(orth);
     };
     if (!use_graph) {
@@ -1217,7 +1221,36 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, sqd_op_s* cache
   SQD_REQUIRE(fn == sqd_op_matvec_cb, "mixed precision needs an sqd operator as the matvec");
   auto* op = static_cast<sqd_op_s*>(ctx);
   op_ensure_values32(op, st);
-  SolverCache<NC>* cache = solver_cache<NC>(op, n);
+  // Orthogonality constraints (excited states): FP32 copies for the sweeps, fresh solver
+  // objects (a cached graph would hold the vectors).
+  std::vector<DevBuf<float>> orth32_bufs;
+  std::vector<const void*> orth32;
+  for (const void* o : orth) {
+    DevBuf<float> b;
+    b.alloc(static_cast<size_t>(n) * NC, st);
+    k_convert<float, double, NC><<<G, 256, 0, st>>>(static_cast<const double*>(o), b.ptr, n);
+    SQD_CHECK_LAUNCH();
+    orth32.push_back(b.ptr);
+    orth32_bufs.push_back(std::move(b));
+  }
+  OpCtx32 own_c32{op, NC == 2 ? SQD_C64 : SQD_F32};
+  OpCtx64 own_c64{op, NC == 2 ? SQD_C128 : SQD_F64};
+  std::unique_ptr<Locg<float, NC>> own32;
+  std::unique_ptr<Locg<double, NC>> own64;
+  Locg<float, NC>* l32 = nullptr;
+  Locg<double, NC>* l64 = nullptr;
+  if (orth.empty()) {
+    SolverCache<NC>* cache = solver_cache<NC>(op, n);
+    if (!cache->l64) cache->l64 = std::make_unique<Locg<double, NC>>(n, op_cb64, &cache->c64, st);
+    if (!cache->l32) cache->l32 = std::make_unique<Locg<float, NC>>(n, op_cb32, &cache->c32, st);
+    l32 = cache->l32.get();
+    l64 = cache->l64.get();
+  } else {
+    own64 = std::make_unique<Locg<double, NC>>(n, op_cb64, &own_c64, st);
+    own32 = std::make_unique<Locg<float, NC>>(n, op_cb32, &own_c32, st);
+    l32 = own32.get();
+    l64 = own64.get();
+  }
   // Phase timing on stderr when SQD_LOCG_TRACE is set (like the reference's debug prints).
   const bool trace = std::getenv("SQD_LOCG_TRACE") != nullptr;
   cudaEvent_t ev[5] = {};
@@ -1231,12 +1264,10 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, sqd_op_s* cache
   constexpr int kStall = 25;
   constexpr int kRestarts = 6;
   int it32 = 0;
-  if (!cache->l64) cache->l64 = std::make_unique<Locg<double, NC>>(n, op_cb64, &cache->c64, st);
-  Locg<double, NC>& L = *cache->l64;
+  Locg<double, NC>& L = *l64;
   L.set_stream(st);
   {
-    if (!cache->l32) cache->l32 = std::make_unique<Locg<float, NC>>(n, op_cb32, &cache->c32, st);
-    Locg<float, NC>& L32 = *cache->l32;
+    Locg<float, NC>& L32 = *l32;
     L32.set_stream(st);
     L32.set_params(0.0, nscale, maxiter, kInnerRtol, 0.0, kStall);
     if (xinit) {
@@ -1246,10 +1277,11 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, sqd_op_s* cache
       k_onehot<float, NC><<<G, 256, 0, st>>>(L32.x(), n, xinit_index);
     }
     SQD_CHECK_LAUNCH();
-    L32.start_implicit();
+    if (!xinit) L32.project_orth(orth32, L32.x(), true, G_NONE);
+    L32.start_implicit(orth32);
     L32.proj_ips();
     for (int k = 0; k < kRestarts; ++k) {
-      L32.loop(orth, maxiter, use_graph, true);
+      L32.loop(orth32, maxiter, use_graph, true);
       if (L32.host().niter >= maxiter || L32.host().rzero) break;
       L32.refresh();
       if (L32.host().converged || L32.host().niter >= maxiter) break;
@@ -1259,15 +1291,23 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, sqd_op_s* cache
     SQD_CHECK_LAUNCH();
     mark(1);
   }
-  // FP64 polish: fast implicit iterations (one FP64 matvec each) with the reference's
-  // residual test; in FP64 the carried products drift by O(eps) only.
   mark(2);
   const int left = std::max(1, maxiter - it32);
   L.set_params(tol < 0 ? eps64 : tol, nscale, left, 0.0, 0.0, 0);
-  L.start_implicit();
-  L.proj_ips();
-  mark(3);
-  L.loop(orth, left, use_graph, true);
+  if (orth.empty()) {
+    // FP64 polish: fast implicit iterations (one FP64 matvec each) with the reference's
+    // residual test; in FP64 the carried products drift by O(eps) only.
+    L.start_implicit();
+    L.proj_ips();
+    mark(3);
+    L.loop(orth, left, use_graph, true);
+  } else {
+    // With constraints: the reference iteration from the FP32 vector, which projects every
+    // residual against the constraint vectors in FP64.
+    L.start(orth);
+    mark(3);
+    L.loop(orth, left, use_graph);
+  }
   const int it64 = L.host().niter;
   mark(4);
   if (trace) {
@@ -1861,7 +1901,6 @@ extern "C" int sqd_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const
     cudaStream_t st = as_stream(stream);
     std::vector<const void*> ov;
     for (int k = 0; k < n_orth; ++k) ov.push_back(orth[k]);
-    SQD_REQUIRE(mode == SQD_LOCG_FP64 || ov.empty(), "mixed precision does not support orth");
     OpDtypeCtx octx{nullptr, dtype};
     sqd_matvec_fn f = fn;
     void* c = ctx;

@@ -56,3 +56,28 @@ def test_cached_solver_follows_coefficient_refresh():
                                                  padded=True), space, cache_strategy=(1, 2))
     e_fresh, _, _ = rq.ground_locg(fresh, x0, mode='mixed')
     assert abs(e_cached - e_fresh) <= 1e-12 * abs(e_fresh)
+
+
+def test_mixed_precision_excited_state_with_orth():
+    """Deflation against the ground state (ground_locg's orth) in the mixed-precision solver:
+    FP32 sweeps project every search direction, the FP64 polish runs the reference iteration."""
+    wl, ham, space = _case(7)
+    op = rq.SQDOperator(ham, space, cache_strategy=(1, 2))
+    ip, ix, dt = op.csr()
+    n = op.size
+    dense = np.zeros((n, n), dtype=np.complex128)
+    ipn, ixn, dtn = ip.cpu().numpy(), ix.cpu().numpy(), dt.cpu().numpy()
+    for r in range(n):
+        dense[r, ixn[ipn[r]:ipn[r + 1]]] += dtn[ipn[r]:ipn[r + 1]]
+    w, u = np.linalg.eigh(dense)
+    assert w[1] - w[0] > 1e-6
+    x0 = torch.as_tensor(wl.start_vector(), device='cuda')
+    orth = (torch.as_tensor(u[:, 0], device='cuda'),)
+    e64, v64, _ = rq.ground_locg(op, x0, orth=orth, mode='fp64', tol=1e-12)
+    e32, v32, _ = rq.ground_locg(op, x0, orth=orth, mode='mixed', tol=1e-12)
+    assert abs(e64 - w[1]) <= 1e-8 * abs(w[1])
+    assert abs(e32 - w[1]) <= 1e-8 * abs(w[1])
+    assert abs(np.vdot(u[:, 0], v32.cpu().numpy())) < 1e-6
+    # the cached solver objects of an unconstrained solve are unaffected
+    e_gs, _, _ = rq.ground_locg(op, x0, mode='mixed')
+    assert abs(e_gs - w[0]) <= 1e-8 * abs(w[0])
