@@ -11,7 +11,7 @@
 // An H or L source is implied by (slab, position), so the elements of those pairs are laid out
 // again as dense slabs and the matvec streams them with coalesced loads and gathers v (or its
 // transpose vT[l][h]) with coalesced loads too, instead of one scattered gather and one index
-// per pair.  One matvec is six launches:
+// per pair.  One matvec is five launches:
 //   1. vT = transpose(v)                                (32 x 32 tiles through shared memory)
 //   2. t2[l][h] = sum_e VL(lo[l] + e, h) vT[l'_e][h]     (L part; FP64 partial)
 //   3. t2' = transpose(t2) into the vT buffer           (now [h][l])
@@ -23,15 +23,20 @@
 // gathered vector stays in L2 while all slabs pass over it.  The elements are stored in the
 // same panel-major order, VH(k, l) at ((l / 32) * KH + k) * 32 + l % 32 (KH = entries of all
 // slabs), so the element stream of a panel pass is one contiguous sweep.  Source indices are
-// kept premultiplied (h' * nl, l' * nh).
+// kept premultiplied (h' * nl, l' * nh).  At 48 qubits the FP64 passes stream their elements
+// at ~5 TB/s while L2 serves one amplitude per entry (~19 TB/s); FP32 passes are bound by the
+// latency of their index -> amplitude chains.
 // Step 4: when all M source slabs of every slab fit in shared memory together (small slabs,
 // e.g. 512 strings per half), k_tail_smem stages them per block and gathers from shared
 // memory through 16-bit indices of a compact copy of the row tails; otherwise (and under
-// SQD_LAYOUT_PRODUCT_CSR) the CSR kernel runs over the row tails, gathering from global memory.  Both slab passes are bound by the L2 -> SM traffic of
-// the coalesced amplitude reads (one amplitude per entry, served by L2) rather than by DRAM.
+// SQD_LAYOUT_PRODUCT_CSR) the CSR kernel runs over the row tails, gathering from global
+// memory.
 // FP32 vectors keep the compensated accumulation in every part and pass partials in FP64, so
 // the result is rounded once.  The elements are the same numbers as in the CSR arrays; only
 // the summation order of a row changes (L and M pairs before H pairs).
+//
+// The file also builds the connectivity itself for such subspaces (op_connect_product): the
+// partners of every string of each half, then each row's pairs assembled from them.
 #include <algorithm>
 #include <climits>
 #include <type_traits>
