@@ -70,14 +70,19 @@ def tune_lanes(op, dtype, candidates=(2, 4, 8, 16, 32), reps=5, chunks=(0, 64, 2
 
 
 def tune_lookup(hamiltonian, space, cache_strategy=(1, 0)):
-    """Builds the operator with each lookup method; returns (best, {method: seconds})."""
+    """Builds the operator with each lookup method ('product' only on product subspaces);
+    returns (best, {method: seconds})."""
     import time
     from .sqd import SQDOperator
+    from ._lib import SQDError
     times = {}
-    for method in ('hash', 'bsearch'):
+    for method in ('hash', 'bsearch', 'product'):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        SQDOperator(hamiltonian, space, cache_strategy, lookup=method)
+        try:
+            SQDOperator(hamiltonian, space, cache_strategy, lookup=method)
+        except SQDError:
+            continue                         # 'product' on a subspace that is not a product
         torch.cuda.synchronize()
         times[method] = time.perf_counter() - t0
     return min(times, key=times.get), times

@@ -48,3 +48,23 @@ def test_invalid_arguments_return_status_without_gpu():
     assert st == _lib.SQD_ERR_INVALID
     with pytest.raises(ValueError):
         _lib.check(st)
+
+
+def header_enums():
+    """name -> value for every `SQD_X = value` enumerator in the header."""
+    text = re.sub(r'/\*.*?\*/', '', open(HEADER).read(), flags=re.S)
+    return {m.group(1): int(m.group(2))
+            for m in re.finditer(r'\b(SQD_[A-Z0-9_]+)\s*=\s*(-?\d+)', text)}
+
+
+def test_python_constants_match_header_enums():
+    enums = header_enums()
+    for name in ('SQD_OK', 'SQD_ERR_INVALID', 'SQD_F64', 'SQD_C128', 'SQD_F32', 'SQD_C64',
+                 'SQD_LOOKUP_HASH', 'SQD_LOOKUP_BSEARCH', 'SQD_LOOKUP_AUTO',
+                 'SQD_LOOKUP_PRODUCT'):
+        assert getattr(_lib, name) == enums[name], name
+    from rqutils_b200.sqd import SQDOperator, _LOOKUPS
+    assert SQDOperator.LAYOUTS == {'csr': enums['SQD_LAYOUT_CSR'],
+                                   'product': enums['SQD_LAYOUT_PRODUCT'],
+                                   'product-csr': enums['SQD_LAYOUT_PRODUCT_CSR']}
+    assert _LOOKUPS['product'] == enums['SQD_LOOKUP_PRODUCT']
