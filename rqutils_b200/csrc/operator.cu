@@ -479,7 +479,8 @@ void op_ensure_values32(sqd_op_s* op, cudaStream_t st) {
     k_to_float<<<grid_for(n, 256, 16384), 256, 0, st>>>(op->values.ptr, op->values32.ptr, n);
     SQD_CHECK_LAUNCH();
   }
-  op_product_values32(op, st);
+  // FP32 slab copies only when FP32 vectors use a product layout.
+  if (op->layout[1] != SQD_LAYOUT_CSR) op_product_values32(op, st);
 }
 
 }  // namespace sqd

@@ -989,7 +989,7 @@ void op_product_build(sqd_op_s* op, cudaStream_t st) {
                                     std::to_string(hbad) + " pairs)");
   }
   build_tail(op, st);
-  if (op->values32.ptr) {
+  if (op->values32.ptr && op->layout[1] != SQD_LAYOUT_CSR) {
     to_float(op->prod.vh, op->prod.vh32, st);
     to_float(op->prod.vl, op->prod.vl32, st);
     if (op->prod.tail_slots) to_float(op->prod.mval, op->prod.mval32, st);
@@ -1088,8 +1088,15 @@ extern "C" int sqd_op_set_layout(sqd_op_t op, int precision, int layout, void* s
       cudaStream_t st = as_stream(stream);
       op_product_build(op, st);
       if (precision == 1) {
-        op_ensure_values32(op, st);
-        SQD_CUDA(cudaStreamSynchronize(st));
+        const int prev = op->layout[1];
+        op->layout[1] = layout;
+        try {
+          op_ensure_values32(op, st);
+          SQD_CUDA(cudaStreamSynchronize(st));
+        } catch (...) {
+          op->layout[1] = prev;
+          throw;
+        }
       }
     }
     op->layout[precision] = layout;
