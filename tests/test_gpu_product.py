@@ -196,3 +196,24 @@ def test_product_lookup_needs_a_product_subspace():
     ref = rq.SQDOperator(ham, space, cache_strategy=(1, 2), lookup='hash')
     v = _vector(ref.size, torch.complex128)
     torch.testing.assert_close(auto.matvec(v), ref.matvec(v), rtol=0, atol=0)
+
+
+def test_product_without_conserved_weights():
+    """Halves of random strings (no conserved weight, so no sector filter): the per-half
+    connectivity still equals the sweep's and the product layout still matches the oracle."""
+    rng = np.random.default_rng(33)
+    hi = np.unique(rng.integers(0, 256, size=40, dtype=np.uint64))
+    lo = np.unique(rng.integers(0, 256, size=30, dtype=np.uint64))
+    states = ((hi[:, None] << np.uint64(8)) | lo[None, :]).reshape(-1)
+    x, z, c = W.random_pauli_sum(16, 300, rng, wmax=3)
+    ham = rq.PauliSumXZ.from_xz(x, z, c, 16, force_real=True, padded=True)
+    space = rq.Subspace.from_u64(states, 16)
+    sweep = rq.SQDOperator(ham, space, cache_strategy=(1, 2), lookup='hash')
+    prod = rq.SQDOperator(ham, space, cache_strategy=(1, 2), lookup='product')
+    for u, w in zip(sweep.csr(), prod.csr()):
+        np.testing.assert_array_equal(u.cpu().numpy(), w.cpu().numpy())
+    v = _vector(prod.size, torch.complex128, seed=4)
+    ref = _oracle_hv(x, z, c, states, 16, v.cpu().numpy(), True)
+    for layout in ('product', 'product-csr'):
+        prod.set_layout(0, layout)
+        assert rel(prod.matvec(v).cpu().numpy(), ref) < MATVEC_RTOL
