@@ -217,3 +217,24 @@ def test_product_without_conserved_weights():
     for layout in ('product', 'product-csr'):
         prod.set_layout(0, layout)
         assert rel(prod.matvec(v).cpu().numpy(), ref) < MATVEC_RTOL
+
+
+def test_product_layout_large_grid_matches_csr():
+    """1024 x 512 product (multi-panel slab passes with many slabs per panel): product layout
+    against the CSR layout, both precisions."""
+    rng = np.random.default_rng(8)
+    hi = np.arange(1024, dtype=np.uint64)
+    lo = np.sort(rng.choice(np.arange(1024, dtype=np.uint64), size=512, replace=False))
+    states = ((hi[:, None] << np.uint64(10)) | lo[None, :]).reshape(-1)
+    x, z, c = W.random_pauli_sum(20, 200, rng, wmax=3)
+    ham = rq.PauliSumXZ.from_xz(x, z, c, 20, force_real=True, padded=True)
+    op = rq.SQDOperator(ham, rq.Subspace.from_u64(states, 20), cache_strategy=(1, 2))
+    info = op.product_info()
+    assert (info['n_high'], info['n_low']) == (1024, 512)
+    for dt, prec, tol in ((torch.complex128, 0, MATVEC_RTOL), (torch.complex64, 1, MATVEC32_RTOL)):
+        v = _vector(op.size, dt, seed=6)
+        op.set_layout(prec, 'csr')
+        ref = op.matvec(v).to(torch.complex128).cpu().numpy()
+        op.set_layout(prec, 'product-csr')
+        got = op.matvec(v).to(torch.complex128).cpu().numpy()
+        assert rel(got, ref) < tol
