@@ -109,7 +109,8 @@ int sqd_space_info(sqd_space_t s, int64_t* n_unique, int64_t* states_size, int* 
 /* Sorted unique states (n_unique values). */
 int sqd_space_states(sqd_space_t s, uint64_t* out, void* stream);
 /* get_xsource (sqd.py:485-548), sorted input: out[states_size] = index j with S[j] == S[i]^x,
- * else -1; fill-in slots get exactly the values the reference's sort-based algorithm gives. */
+ * else -1; fill-in slots get exactly the values the reference's sort-based algorithm gives.
+ * lookup: SQD_LOOKUP_HASH or SQD_LOOKUP_BSEARCH (SQD_LOOKUP_AUTO means the hash table). */
 int sqd_xsource(sqd_space_t s, uint64_t x, int lookup, int32_t* out, void* stream);
 void sqd_space_destroy(sqd_space_t s);
 

@@ -293,12 +293,14 @@ extern "C" int sqd_space_states(sqd_space_t s, uint64_t* out, void* stream) {
 extern "C" int sqd_xsource(sqd_space_t s, uint64_t x, int lookup, int32_t* out, void* stream) {
   return guarded([&] {
     SQD_REQUIRE(s != nullptr && out != nullptr, "NULL argument");
-    SQD_REQUIRE(lookup == SQD_LOOKUP_HASH || lookup == SQD_LOOKUP_BSEARCH, "bad lookup method");
+    SQD_REQUIRE(lookup == SQD_LOOKUP_HASH || lookup == SQD_LOOKUP_BSEARCH ||
+                    lookup == SQD_LOOKUP_AUTO,
+                "sqd_xsource takes SQD_LOOKUP_HASH, SQD_LOOKUP_BSEARCH or SQD_LOOKUP_AUTO");
     SQD_REQUIRE((x & ~s->fill_state) == 0, "x has bits above num_qubits");
     cudaStream_t st = as_stream(stream);
     k_xsource<<<grid_for(s->states_size, 256, 8192), 256, 0, st>>>(
         s->states.ptr, s->n_unique, s->states_size, x, s->hkeys.ptr, s->hvals.ptr, s->hmask,
-        lookup, out);
+        lookup == SQD_LOOKUP_BSEARCH ? SQD_LOOKUP_BSEARCH : SQD_LOOKUP_HASH, out);
     SQD_CHECK_LAUNCH();
   });
 }
