@@ -154,3 +154,32 @@ def test_oracle_reproduces_golden_fixtures(name):
             np.testing.assert_allclose(b, a, rtol=1e-12, atol=1e-12, err_msg=key)
         else:
             np.testing.assert_array_equal(b, a, err_msg=key)
+
+
+def test_product_subspace_source_structure():
+    """The invariant behind the product layout and the per-half connectivity, checked with the
+    literal sort-based get_xsource (sqd.py:485-548): in an alpha x beta product subspace a
+    group acting on one half has a source exactly when that half's string has a partner, and
+    the source keeps the other half; a group acting on both halves needs both partners."""
+    wl = W.jw_workload('t', 6, 2, 9, 11, 5)
+    n, half = wl.num_qubits, wl.num_qubits // 2
+    lo_mask = np.uint64((1 << half) - 1)
+    states = np.sort(wl.states)
+    sp = OQ.pack_states(OQ.u64_to_states(states, n))
+    his = np.unique(states >> np.uint64(half))
+    los = np.unique(states & lo_mask)
+    nl = los.shape[0]
+    assert his.shape[0] * nl == states.shape[0]
+    oham = OS.from_paulisum((wl.labels, list(wl.coeffs)), force_real=True, add_padding=True)
+    for xpacked in oham.x:
+        src = OQ.get_xsource(xpacked, sp)[:states.shape[0]]
+        x = int(OQ.packed_to_u64(xpacked[None, :], n)[0])
+        xh, xl = x >> half, x & int(lo_mask)
+        for r, s in enumerate(states):
+            h, l = r // nl, r % nl
+            ph = np.searchsorted(his, (int(s) >> half) ^ xh)
+            pl = np.searchsorted(los, (int(s) & int(lo_mask)) ^ xl)
+            ok_h = ph < his.shape[0] and his[ph] == ((int(s) >> half) ^ xh)
+            ok_l = pl < nl and los[pl] == ((int(s) & int(lo_mask)) ^ xl)
+            expect = ph * nl + pl if (ok_h and ok_l) else -1
+            assert src[r] == expect
