@@ -338,6 +338,7 @@ def run_ours(args):
     extra = {}
     if not args.no_locg and rank == 0:
         extra['locg'] = locg_times(rq, op, wl, dev, use_graph=not args.no_graph)
+        extra['locg']['bytes_per_iteration'] = locg_bytes(n_rows, m_terms, j_groups, nnz)
     if args.workload == 'c5' and rank == 0:
         extra['gradient'] = gradient_check(rq, op, wl)
     line = None
@@ -458,6 +459,17 @@ def gradient_check(rq, op, wl, n_coords=32, h=1e-5):
             'time_energy_and_gradient_s': t_grad, 'fd_coords': int(n_coords), 'fd_step': h,
             'fd_time_s': t_fd, 'max_rel_err_vs_fd': float(max(errs)),
             'median_rel_err_vs_fd': float(np.median(errs))}
+
+
+def locg_bytes(n, m, j, p):
+    """Algorithmic bytes of one LOCG iteration: matvecs x the matvec formula (W = 1, w_c = 16)
+    plus the vector reads and writes of the fused passes, counted from the iteration bodies:
+    the FP64 reference iteration (ground_locg.py:324-383) makes 4 complex128 matvecs and 42
+    vector reads/writes; an FP32 sweep of the mixed solver 1 complex64 matvec and 33."""
+    def mv(w_v):
+        return n * (8 + 2 * w_v) + p * w_v + m * (8 + 16) + j * 8
+    return {'fp64': 4 * mv(16) + 42 * n * 16, 'fp32_sweep': mv(8) + 33 * n * 8,
+            'formula': '#matvecs * (N(8W+2w_v) + P w_v + M(8W+w_c) + 8WJ) + #vector passes * N w_v'}
 
 
 def locg_times(rq, op, wl, dev, use_graph=True):
