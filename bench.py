@@ -334,6 +334,10 @@ def run_ours(args):
     peak, peak_kind = load_peaks()
     achieved = bytes_alg / (t_local / args.steps) / 1e9
     traffic = load_traffic(args.workload, cache, layout)
+    props = torch.cuda.get_device_properties(dev)
+    sm_mhz = clocks['sm_mhz'] if clocks and clocks.get('sm_mhz') else 1965.0
+    issue = issue_bound(n_rows, m_terms, nnz, op.value_complex, props.multi_processor_count,
+                        sm_mhz, t_local / args.steps)
 
     extra = {}
     if not args.no_locg and rank == 0:
@@ -363,6 +367,7 @@ def run_ours(args):
                          'formula': 'N(8W+2w_v) + P_valid w_v + M(8W+w_c) + J 8W, W=1, '
                                     'w_v=16, w_c=16, P_valid = stored pairs',
                          'timed': 'one whole FP64 matvec (all its kernels) per launch'},
+            'issue_bound': issue,
             'e2e': {'value': e2e_value, 'unit': UNIT,
                     'h2d_bytes_per_step': int(v.numel() * 16),
                     'd2h_bytes_per_step': int(v.numel() * 16)},
@@ -459,6 +464,31 @@ def gradient_check(rq, op, wl, n_coords=32, h=1e-5):
             'time_energy_and_gradient_s': t_grad, 'fd_coords': int(n_coords), 'fd_step': h,
             'fd_time_s': t_fd, 'max_rel_err_vs_fd': float(max(errs)),
             'median_rel_err_vs_fd': float(np.median(errs))}
+
+
+POPC_PER_SM_CLK = 16      # 32-bit population count results per SM per clock (sm_90/sm_100)
+DFMA_PER_SM_CLK = 64      # FP64 fused multiply-adds per SM per clock (B200: 148 SMs, ~37 TF/s)
+
+
+def issue_bound(n, m, p, value_complex, sms, sm_mhz, t_matvec_s):
+    """Instruction-issue floors of one FP64 matvec, beside its memory roofline.
+
+    The reference's matvec (apply_h_x_cached, sqd.py:694-709) recomputes every group's diagonal
+    (get_diagonal, sqd.py:603-628) for every row and merged term: N x M population counts per
+    matvec.  The timed kernels read cached elements instead: one FP64 complex-by-real (2 FMAs)
+    or complex-by-complex (4 FMAs) product per stored pair.  Both are divided by the nominal
+    per-SM throughputs at the sampled SM clock."""
+    hz = sms * sm_mhz * 1e6
+    popc = n * m
+    fma = p * (4 if value_complex else 2)
+    return {'reference_popcounts_per_matvec': popc,
+            'reference_popcount_floor_ms': popc / (POPC_PER_SM_CLK * hz) * 1e3,
+            'cached_fp64_fma_per_matvec': fma,
+            'cached_fp64_fma_floor_ms': fma / (DFMA_PER_SM_CLK * hz) * 1e3,
+            'timed_matvec_ms': t_matvec_s * 1e3,
+            'sms': sms, 'sm_mhz': sm_mhz,
+            'rates': f'nominal: {POPC_PER_SM_CLK} popc and {DFMA_PER_SM_CLK} FP64 FMA '
+                     'per SM per clock'}
 
 
 def locg_bytes(n, m, j, p):

@@ -30,3 +30,17 @@ def test_workload_names_and_configs():
     cfg = bench.workload_config(wl, (1, 2))
     assert cfg['subspace_dim'] == 2000 and cfg['num_qubits'] == 16
     assert 'random Pauli sum' in cfg['workload']
+
+
+def test_issue_bound_estimate():
+    # C3 shape: the reference's on-the-fly diagonals would be popcount-bound at ~1.75 s per
+    # matvec, the cached FP64 elements need well under the measured 6 ms of FP64 FMAs
+    n, m, p = 16777216, 485281, 2653787580
+    b = bench.issue_bound(n, m, p, False, 148, 1965.0, 6.0e-3)
+    assert b['reference_popcounts_per_matvec'] == n * m
+    assert abs(b['reference_popcount_floor_ms'] - n * m / (16 * 148 * 1965e6) * 1e3) < 1e-9
+    assert 1500 < b['reference_popcount_floor_ms'] < 2000
+    assert b['cached_fp64_fma_per_matvec'] == 2 * p
+    assert b['cached_fp64_fma_floor_ms'] < 0.1 * b['timed_matvec_ms']
+    assert bench.issue_bound(n, m, p, True, 148, 1965.0, 6.0e-3)['cached_fp64_fma_per_matvec'] \
+        == 4 * p
