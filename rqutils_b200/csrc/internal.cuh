@@ -82,12 +82,16 @@ struct ProductLayout {
   sqd::DevBuf<double> vh, vl;        // FP64 elements (x2 interleaved when complex)
   sqd::DevBuf<float> vh32, vl32;     // FP32 copies
   sqd::DevBuf<double> vt, tt, t;     // per-matvec scratch: transposed input, L and M partials
-  // M pairs gathered from shared memory, built when every slab's M source slabs fit there
-  // together: compact copies of the row tails (mptr, mval) whose sources are indices into the
-  // block's staged slabs (msidx = slot * nl + l'), and each slab's source slabs (slist).
+  // Compact copies of the row tails (the M pairs of each row, contiguous: mptr, mval) with the
+  // sources in one or both of two forms.  Shared memory (tail_slots > 0), when every slab's M
+  // source slabs fit there together: indices into the block's staged slabs (msidx = slot * nl +
+  // l'), and each slab's source slabs are listed (slist).  Short tails (compact_tail): rows
+  // (mcol), read by the CSR tail kernel.
   int tail_slots = 0;                // largest number of M source slabs of one slab
+  int compact_tail = 0;
   sqd::DevBuf<int64_t> mptr;         // [n + 1]
-  sqd::DevBuf<uint16_t> msidx;       // [pairs_m]
+  sqd::DevBuf<uint16_t> msidx;       // [pairs_m] (shared-memory form)
+  sqd::DevBuf<uint32_t> mcol;        // [pairs_m] (short-tail form)
   sqd::DevBuf<double> mval;          // [pairs_m] (x2 interleaved when complex)
   sqd::DevBuf<float> mval32;
   sqd::DevBuf<int64_t> soff;         // [nh + 1]

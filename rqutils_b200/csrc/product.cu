@@ -273,9 +273,11 @@ k_slab(int64_t A, int64_t B, int64_t total_k, int64_t a_tiles, const int64_t* __
   }
 }
 
-// M pairs of every row (the CSR tail after the row's H and L entries), FP64 partial per row.
-// Same schedule as the CSR matvec: LPR lanes per row, interleaved or chunked rows.
-template <typename R, int NCV, int NCA, int LPR>
+// M pairs of every row, FP64 partial per row.  Same schedule as the CSR matvec: LPR lanes per
+// row, interleaved or chunked rows.  The pairs are the row's CSR tail after its H and L entries
+// (row_ptr, cols, vals: the operator's arrays; ho, lo give the H and L counts) or, COMPACT, the
+// contiguous copy of the tails (row_ptr = mptr, cols = mcol, vals = mval; ho, lo unused).
+template <typename R, int NCV, int NCA, int LPR, bool COMPACT>
 __global__ void __launch_bounds__(256)
 k_mv_mixed(const int64_t* __restrict__ row_ptr, const uint32_t* __restrict__ cols,
            const R* __restrict__ vals, const R* __restrict__ v, const int64_t* __restrict__ ho,
@@ -288,10 +290,12 @@ k_mv_mixed(const int64_t* __restrict__ row_ptr, const uint32_t* __restrict__ col
     const int64_t row = rb + slot;
     CAcc<R, NCV, NCA> acc;
     if (row < lim) {
-      const int64_t h = row / nl, l = row - h * nl;
-      const int64_t skip =
-          (__ldg(ho + h + 1) - __ldg(ho + h)) + (__ldg(lo + l + 1) - __ldg(lo + l));
-      const int64_t b = __ldg(row_ptr + row) + skip, e = __ldg(row_ptr + row + 1);
+      int64_t b = __ldg(row_ptr + row);
+      const int64_t e = __ldg(row_ptr + row + 1);
+      if constexpr (!COMPACT) {
+        const int64_t h = row / nl, l = row - h * nl;
+        b += (__ldg(ho + h + 1) - __ldg(ho + h)) + (__ldg(lo + l + 1) - __ldg(lo + l));
+      }
       csr_row_dot<R, NCV, NCA, LPR>(cols, vals, v, b + sub, e, acc);
     }
     acc.merge(LPR);
@@ -321,7 +325,8 @@ __device__ __forceinline__ int64_t tail_begin(const int64_t* row_ptr, const int6
   return row_ptr[r] + (ho[h + 1] - ho[h]) + (lo[l + 1] - lo[l]);
 }
 
-// bits[h][h' / 32] |= 1 << (h' % 32) for every M source slab h' of slab h; per-row tail lengths.
+// Per-row tail lengths and, when bits is given, bits[h][h' / 32] |= 1 << (h' % 32) for every M
+// source slab h' of slab h.
 __global__ void k_tail_mark(const int64_t* __restrict__ row_ptr, const uint32_t* __restrict__ cols,
                             const int64_t* __restrict__ ho, const int64_t* __restrict__ lo,
                             int64_t n, int64_t nl, int64_t words, uint32_t* bits, int64_t* len) {
@@ -330,6 +335,7 @@ __global__ void k_tail_mark(const int64_t* __restrict__ row_ptr, const uint32_t*
     const int64_t h = r / nl;
     const int64_t b = tail_begin(row_ptr, ho, lo, r, nl), e = row_ptr[r + 1];
     len[r] = e - b;
+    if (bits == nullptr) continue;
     for (int64_t i = b; i < e; ++i) {
       const uint32_t hs = static_cast<uint32_t>(cols[i] / nl);
       atomicOr(bits + h * words + (hs >> 5), 1u << (hs & 31));
@@ -364,14 +370,15 @@ __global__ void k_tail_slist(const uint32_t* __restrict__ bits, int64_t nh, int6
   }
 }
 
-// Compact tail copy: element and shared-memory index (slot of h' among h's sources).
+// Compact tail copy: the element, and the source row (mcol, when given) or the shared-memory
+// index (slot of h' among h's sources; with_index).
 template <int NCA>
 __global__ void k_tail_fill(const int64_t* __restrict__ row_ptr, const uint32_t* __restrict__ cols,
                             const double* __restrict__ vals, const int64_t* __restrict__ ho,
                             const int64_t* __restrict__ lo, const uint32_t* __restrict__ bits,
                             int64_t n, int64_t nl, int64_t words,
                             const int64_t* __restrict__ mptr, uint16_t* msidx, double* mval,
-                            int with_index) {
+                            int with_index, uint32_t* mcol) {
   for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n;
        r += int64_t(gridDim.x) * blockDim.x) {
     const int64_t h = r / nl;
@@ -380,6 +387,7 @@ __global__ void k_tail_fill(const int64_t* __restrict__ row_ptr, const uint32_t*
     for (int64_t i = b; i < e; ++i, ++j) {
 #pragma unroll
       for (int t = 0; t < NCA; ++t) mval[NCA * j + t] = vals[NCA * i + t];
+      if (mcol != nullptr) mcol[j] = cols[i];
       if (!with_index) continue;
       const int64_t c = cols[i];
       const int64_t hs = c / nl;
@@ -536,23 +544,33 @@ void to_float(const DevBuf<double>& in, DevBuf<float>& out, cudaStream_t st) {
   SQD_CHECK_LAUNCH();
 }
 
-// Builds the shared-memory form of the M pairs when every slab's M source slabs fit in
-// kTailSmemMax together (at 8 bytes per amplitude) and 16-bit indices reach them.
-void build_tail(sqd_op_s* op, cudaStream_t st) {
+// A row tail read in place is a short segment of the row's long pair list (C3-like subspaces:
+// ~11 M pairs among ~160), so its element and source loads use few bytes of the sectors they
+// fetch.  Tails up to this many pairs per row on average are also copied contiguously.
+constexpr int64_t kCompactTailMax = 32;
+
+// Shared-memory form of the M pairs, when every slab's M source slabs fit in kTailSmemMax
+// together (at 8 bytes per amplitude) and 16-bit indices reach them.  Fills len (per-row tail
+// lengths) either way; returns whether the form was built.
+bool build_tail_smem(sqd_op_s* op, DevBuf<int64_t>& len, cudaStream_t st) {
   ProductLayout& L = op->prod;
   const int64_t nh = L.nh, nl = L.nl, n = nh * nl;
-  if (L.pairs_m <= 0 || nh > 65536) return;
+  const unsigned G = grid_for(n, 256, 16384);
+  if (nh > 65536) {
+    k_tail_mark<<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, L.ho.ptr, L.lo.ptr, n, nl, 0,
+                                   nullptr, len.ptr);
+    SQD_CHECK_LAUNCH();
+    return false;
+  }
   const int64_t words = (nh + 31) / 32;
   DevBuf<uint32_t> bits;
   bits.alloc(static_cast<size_t>(nh * words), st);
   SQD_CUDA(cudaMemsetAsync(bits.ptr, 0, sizeof(uint32_t) * nh * words, st));
-  DevBuf<int64_t> len, counts;
-  len.alloc(n, st);
+  DevBuf<int64_t> counts;
   counts.alloc(nh, st);
   DevBuf<unsigned> maxc;
   maxc.alloc(1, st);
   SQD_CUDA(cudaMemsetAsync(maxc.ptr, 0, sizeof(unsigned), st));
-  const unsigned G = grid_for(n, 256, 16384);
   k_tail_mark<<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, L.ho.ptr, L.lo.ptr, n, nl, words,
                                  bits.ptr, len.ptr);
   SQD_CHECK_LAUNCH();
@@ -562,7 +580,7 @@ void build_tail(sqd_op_s* op, cudaStream_t st) {
   unsigned slots = 0;
   copy_to_host(&slots, maxc.ptr, 1, st);
   const int64_t span = static_cast<int64_t>(slots) * nl;
-  if (slots == 0 || span > 65535 || static_cast<size_t>(span) * 8 > kTailSmemMax) return;
+  if (slots == 0 || span > 65535 || static_cast<size_t>(span) * 8 > kTailSmemMax) return false;
   L.soff.alloc(nh + 1, st);
   exclusive_scan_i64(counts.ptr, L.soff.ptr, nh, true, st);
   int64_t total = 0;
@@ -579,31 +597,64 @@ void build_tail(sqd_op_s* op, cudaStream_t st) {
   if (nca == 2)
     k_tail_fill<2><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, op->values.ptr, L.ho.ptr,
                                       L.lo.ptr, bits.ptr, n, nl, words, L.mptr.ptr, L.msidx.ptr,
-                                      L.mval.ptr, 1);
+                                      L.mval.ptr, 1, nullptr);
   else
     k_tail_fill<1><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, op->values.ptr, L.ho.ptr,
                                       L.lo.ptr, bits.ptr, n, nl, words, L.mptr.ptr, L.msidx.ptr,
-                                      L.mval.ptr, 1);
+                                      L.mval.ptr, 1, nullptr);
   SQD_CHECK_LAUNCH();
   allow_tail_smem_all();
   SQD_CUDA(cudaStreamSynchronize(st));
   L.tail_slots = static_cast<int>(slots);
+  return true;
 }
 
-// Tail elements again after a coefficient update (indices unchanged).
+// Compact forms of the M pairs: the shared-memory form where it applies, and the short-tail
+// form (source rows beside the same contiguous elements, for the CSR tail kernel) when the
+// tails average at most kCompactTailMax pairs per row.  Longer tails are read in place.
+void build_tail(sqd_op_s* op, cudaStream_t st) {
+  ProductLayout& L = op->prod;
+  const int64_t n = L.nh * L.nl;
+  if (L.pairs_m <= 0) return;
+  DevBuf<int64_t> len;
+  len.alloc(n, st);
+  const bool smem = build_tail_smem(op, len, st);
+  if (L.pairs_m > kCompactTailMax * n) return;
+  const int nca = op->value_complex ? 2 : 1;
+  if (!smem) {
+    L.mptr.alloc(n + 1, st);
+    exclusive_scan_i64(len.ptr, L.mptr.ptr, n, true, st);
+    L.mval.alloc(static_cast<size_t>(L.pairs_m) * nca, st);
+  }
+  L.mcol.alloc(static_cast<size_t>(L.pairs_m), st);
+  const unsigned G = grid_for(n, 256, 16384);
+  if (nca == 2)
+    k_tail_fill<2><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, op->values.ptr, L.ho.ptr,
+                                      L.lo.ptr, nullptr, n, L.nl, 0, L.mptr.ptr, nullptr,
+                                      L.mval.ptr, 0, L.mcol.ptr);
+  else
+    k_tail_fill<1><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, op->values.ptr, L.ho.ptr,
+                                      L.lo.ptr, nullptr, n, L.nl, 0, L.mptr.ptr, nullptr,
+                                      L.mval.ptr, 0, L.mcol.ptr);
+  SQD_CHECK_LAUNCH();
+  SQD_CUDA(cudaStreamSynchronize(st));
+  L.compact_tail = 1;
+}
+
+// Tail elements again after a coefficient update (sources unchanged).
 void refill_tail(sqd_op_s* op, cudaStream_t st) {
   ProductLayout& L = op->prod;
-  if (!L.tail_slots) return;
+  if (L.mval.ptr == nullptr) return;
   const int64_t n = L.nh * L.nl;
   const unsigned G = grid_for(n, 256, 16384);
   if (op->value_complex)
     k_tail_fill<2><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, op->values.ptr, L.ho.ptr,
                                       L.lo.ptr, nullptr, n, L.nl, 0, L.mptr.ptr, nullptr,
-                                      L.mval.ptr, 0);
+                                      L.mval.ptr, 0, nullptr);
   else
     k_tail_fill<1><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, op->values.ptr, L.ho.ptr,
                                       L.lo.ptr, nullptr, n, L.nl, 0, L.mptr.ptr, nullptr,
-                                      L.mval.ptr, 0);
+                                      L.mval.ptr, 0, nullptr);
   SQD_CHECK_LAUNCH();
 }
 
@@ -992,7 +1043,7 @@ void op_product_build(sqd_op_s* op, cudaStream_t st) {
   if (op->values32.ptr && op->layout[1] != SQD_LAYOUT_CSR) {
     to_float(op->prod.vh, op->prod.vh32, st);
     to_float(op->prod.vl, op->prod.vl32, st);
-    if (op->prod.tail_slots) to_float(op->prod.mval, op->prod.mval32, st);
+    if (op->prod.mval.ptr) to_float(op->prod.mval, op->prod.mval32, st);
   }
   op->prod.built = 1;
   SQD_CUDA(cudaStreamSynchronize(st));
@@ -1006,7 +1057,7 @@ void op_product_values(sqd_op_s* op, cudaStream_t st) {
   if (op->prod.vh32.ptr) {
     to_float(op->prod.vh, op->prod.vh32, st);
     to_float(op->prod.vl, op->prod.vl32, st);
-    if (op->prod.tail_slots) to_float(op->prod.mval, op->prod.mval32, st);
+    if (op->prod.mval.ptr) to_float(op->prod.mval, op->prod.mval32, st);
   }
 }
 
@@ -1014,7 +1065,7 @@ void op_product_values32(sqd_op_s* op, cudaStream_t st) {
   if (!op->prod.built || op->prod.vh32.ptr) return;
   to_float(op->prod.vh, op->prod.vh32, st);
   to_float(op->prod.vl, op->prod.vl32, st);
-  if (op->prod.tail_slots) to_float(op->prod.mval, op->prod.mval32, st);
+  if (op->prod.mval.ptr) to_float(op->prod.mval, op->prod.mval32, st);
 }
 
 void op_product_matvec(sqd_op_s* op, const void* v, void* out, int dtype, cudaStream_t st) {
@@ -1055,11 +1106,21 @@ void op_product_matvec(sqd_op_s* op, const void* v, void* out, int dtype, cudaSt
     if (L.pairs_m > 0) {
       if (op->layout[prec] == SQD_LAYOUT_PRODUCT_CSR ||
           !launch_tail_smem<R, NCV, NCA>(op, prec, vin, st)) {
+        const R* MV = nullptr;  // the short-tail copy's elements, when it exists
+        if (L.compact_tail) {
+          if constexpr (sizeof(R) == 8) MV = L.mval.ptr;
+          else MV = L.mval32.ptr;
+        }
         dispatch_lpr(op->lanes_per_row[prec], [&](auto lpr_t) {
           constexpr int LPR = decltype(lpr_t)::value;
-          k_mv_mixed<R, NCV, NCA, LPR><<<mixed_grid(n, LPR), 256, 0, st>>>(
-              op->row_ptr.ptr, op->cols.ptr, VC, vin, L.ho.ptr, L.lo.ptr, nl, L.t.ptr, n,
-              op->chunk_rows[prec]);
+          if (MV != nullptr)
+            k_mv_mixed<R, NCV, NCA, LPR, true><<<mixed_grid(n, LPR), 256, 0, st>>>(
+                L.mptr.ptr, L.mcol.ptr, MV, vin, nullptr, nullptr, nl, L.t.ptr, n,
+                op->chunk_rows[prec]);
+          else
+            k_mv_mixed<R, NCV, NCA, LPR, false><<<mixed_grid(n, LPR), 256, 0, st>>>(
+                op->row_ptr.ptr, op->cols.ptr, VC, vin, L.ho.ptr, L.lo.ptr, nl, L.t.ptr, n,
+                op->chunk_rows[prec]);
           SQD_CHECK_LAUNCH();
         });
       }

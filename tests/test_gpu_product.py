@@ -238,3 +238,31 @@ def test_product_layout_large_grid_matches_csr():
         op.set_layout(prec, 'product-csr')
         got = op.matvec(v).to(torch.complex128).cpu().numpy()
         assert rel(got, ref) < tol
+
+
+@pytest.mark.parametrize('seed, short', [(0, True), (2, False)])
+def test_product_csr_tail_forms(seed, short):
+    """Two-half pairs on the CSR tail kernel: a contiguous copy of the row tails when they are
+    short (at most 32 pairs per row on average; seed 0: 31.8), the tails read in place inside the
+    rows' pair lists otherwise (seed 2: 39.0).  Both against the oracle, every schedule, and after
+    a coefficient refresh."""
+    wl = _jw_small(seed)
+    n = wl.num_qubits
+    ham = rq.PauliSumXZ.from_xz(wl.x, wl.z, wl.coeffs, n, force_real=True, padded=True)
+    op = rq.SQDOperator(ham, rq.Subspace.from_u64(wl.states, n), cache_strategy=(1, 2))
+    for prec in (0, 1):
+        op.set_layout(prec, 'product-csr')
+    assert (op.product_info()['pairs_mixed'] <= 32 * op.size) == short
+    for coeffs in (wl.coeffs, wl.coeffs * 0.7 - 0.01):
+        if coeffs is not wl.coeffs:
+            ham.set_coeffs(torch.as_tensor(coeffs))
+            op.refresh()
+        v = _vector(op.size, torch.complex128, seed=seed + 1)
+        ref = _oracle_hv(wl.x, wl.z, coeffs, wl.states, n, v.cpu().numpy(), True)
+        for prec, dt, tol in ((0, torch.complex128, MATVEC_RTOL),
+                              (1, torch.complex64, MATVEC32_RTOL)):
+            for lanes in (1, 4, 32):
+                for chunk in (0, 64):
+                    op.set_lanes(prec, lanes)
+                    op.set_chunk(prec, chunk)
+                    assert rel(op.matvec(v.to(dt)).cpu().numpy(), ref) < tol
