@@ -585,9 +585,12 @@ __global__ void __launch_bounds__(LC_THREADS) k_lcs(LCArgs<6, 10, 5> a) {
 #pragma unroll
   for (int d = 0; d < NDA; ++d) acc[d][0] = acc[d][1] = 0.0;
   // One element per thread per step (U > 1 makes the compiler keep every coefficient of the
-  // wide shapes in registers; they then spill).
+  // wide shapes in registers; they then spill).  Once this step's loads are issued, the sources
+  // of the thread's next element are prefetched into L2, so two steps' reads are in flight at
+  // the register cost of one.
   constexpr int U = 1;
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  constexpr int64_t EB = int64_t(sizeof(R)) * NC;  // bytes per vector element
   for (int64_t i0 = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i0 < a.n; i0 += U * stride) {
     Cx<R> raw[U][NS];
 #pragma unroll
@@ -597,6 +600,12 @@ __global__ void __launch_bounds__(LC_THREADS) k_lcs(LCArgs<6, 10, 5> a) {
       for (int k = 0; k < NS; ++k)
         raw[u][k] = i < a.n ? ld_elem_rw<R, NC>(static_cast<const R*>(a.src[k]), i)
                             : cx_make<R>(R(0), R(0));
+    }
+    if (i0 + U * stride < a.n) {
+#pragma unroll
+      for (int k = 0; k < NS; ++k)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(static_cast<const char*>(a.src[k]) +
+                                                       (i0 + U * stride) * EB));
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
