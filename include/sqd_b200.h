@@ -112,6 +112,12 @@ int sqd_space_states(sqd_space_t s, uint64_t* out, void* stream);
  * else -1; fill-in slots get exactly the values the reference's sort-based algorithm gives.
  * lookup: SQD_LOOKUP_HASH or SQD_LOOKUP_BSEARCH (SQD_LOOKUP_AUTO means the hash table). */
 int sqd_xsource(sqd_space_t s, uint64_t x, int lookup, int32_t* out, void* stream);
+/* Sorted index of arbitrary keys: out[i] = j with S[j] == keys[i], else -1 (also for keys with
+ * bits above num_qubits).  Replaces the index bookkeeping of get_xsource(sorted_input=False)
+ * (sqd.py:515-516, 542-545: positions of unsorted input rows in the sorted list) and of
+ * uniquify_states(return_indices=True) (sqd.py:478-481).  lookup as in sqd_xsource. */
+int sqd_space_lookup(sqd_space_t s, const uint64_t* keys, int64_t n, int lookup, int32_t* out,
+                     void* stream);
 void sqd_space_destroy(sqd_space_t s);
 
 /* ---------------------------------------------------------------- operator ----------------- */

@@ -31,19 +31,23 @@ def uniquify_states(states_p, states_size, return_indices=False):
     """Restates ``uniquify_states`` (sqd.py:445-482).
 
     Lexicographic sort of the packed rows, unique rows kept in sorted order, tail filled with
-    rows of 255 up to ``states_size``.
+    rows of 255 up to ``states_size`` (a smaller ``states_size`` keeps the first unique rows:
+    the bincount at :465-470 has that length).  The kept position of each unique row is the
+    LAST of its run in the stable sort (cumsum of the per-id counts over positions 1..N-1,
+    :463-470), so ``return_indices`` gives each row's last input occurrence.
     """
     keys = tuple(states_p[:, b] for b in range(states_p.shape[1] - 1, -1, -1))
     perm = np.lexsort(keys)                                  # stable multi-key sort (:457-458)
     states_srt = states_p[perm]
     is_unique = np.any(states_srt[1:] != states_srt[:-1], axis=1)   # :461
-    first = np.concatenate([[True], is_unique])
-    uniq = states_srt[first]
+    last = np.concatenate([is_unique, [True]])               # position i ends its run
+    uniq = states_srt[last]
+    m = min(uniq.shape[0], states_size)
     out = np.full((states_size, states_p.shape[1]), 255, dtype=np.uint8)
-    out[:uniq.shape[0]] = uniq
+    out[:m] = uniq[:m]
     if return_indices:
         idx = np.full(states_size, -1, dtype=np.int64)
-        idx[:uniq.shape[0]] = perm[first]
+        idx[:m] = perm[last][:m]
         return out, idx
     return out
 
@@ -69,6 +73,22 @@ def get_xsource(xsignature, states_p):
     out = np.full(size, -1, dtype=np.int64)
     ok = tposition < source_idx.shape[0]
     out[ok] = source_idx[tposition[ok]]
+    return out.astype(np.int32)
+
+
+def get_xsource_unsorted(xsignature, states_p):
+    """Restates the ``sorted_input=False`` branch of ``get_xsource`` (sqd.py:515-516, 542-545):
+    uniquify with indices, the sorted-input algorithm, then
+    ``arange(N).at[sort_indices].set(sort_indices[xsource])`` with -1 for missing sources.
+    Unique rows without fill rows only (with repeats the reference scatters several values to
+    one position, which JAX leaves unspecified)."""
+    size = states_p.shape[0]
+    srt, sort_indices = uniquify_states(states_p, size, return_indices=True)
+    assert (sort_indices >= 0).all(), 'unique rows without fill rows only'
+    xs = get_xsource(xsignature, srt).astype(np.int64)
+    vals = np.where((xs >= 0) & (xs < size), sort_indices[np.clip(xs, 0, size - 1)], -1)
+    out = np.arange(size, dtype=np.int64)
+    out[sort_indices] = vals
     return out.astype(np.int32)
 
 

@@ -44,6 +44,7 @@ PROTOTYPES = {
                               _c.POINTER(_u64)]),
     'sqd_space_states': (_i32, [_vp, _vp, _vp]),
     'sqd_xsource': (_i32, [_vp, _u64, _i32, _vp, _vp]),
+    'sqd_space_lookup': (_i32, [_vp, _vp, _i64, _i32, _vp, _vp]),
     'sqd_space_destroy': (None, [_vp]),
     'sqd_op_create': (_i32, [_vp, _vp, _i32, _i32, _i32, _vp, _c.POINTER(_vp)]),
     'sqd_op_info': (_i32, [_vp, _c.POINTER(_i64), _c.POINTER(_i64), _c.POINTER(_i32)]),

@@ -8,6 +8,8 @@
 //    an open-addressing hash table, conserved-weight sectors and sector bitmaps.
 //  * sqd_xsource: get_xsource (sqd.py:485-548) for one X mask, bit-exact including the values
 //    the reference's sort-based algorithm produces for fill-in slots.
+//  * sqd_space_lookup: sorted index of arbitrary keys, for the unsorted-input branch of
+//    get_xsource (sqd.py:515-516, 542-545) and the indices of uniquify_states (sqd.py:478-481).
 #include "internal.cuh"
 
 namespace sqd {
@@ -126,6 +128,23 @@ __global__ void k_xsource(const uint64_t* __restrict__ states, int64_t n_unique,
     } else {
       r = (x == 0) ? n_unique : -1;
     }
+    out[i] = static_cast<int32_t>(r);
+  }
+}
+
+// Row index of arbitrary keys: -1 when absent or when a key has bits above num_qubits.
+__global__ void k_lookup_keys(const uint64_t* __restrict__ q, int64_t n, uint64_t valid,
+                              const uint64_t* __restrict__ states, int64_t n_unique,
+                              const uint64_t* __restrict__ hkeys,
+                              const uint32_t* __restrict__ hvals, uint64_t hmask, int lookup,
+                              int32_t* __restrict__ out) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n;
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const uint64_t key = __ldg(q + i);
+    int64_t r = -1;
+    if ((key & ~valid) == 0)
+      r = (lookup == SQD_LOOKUP_BSEARCH) ? bsearch_lookup(states, n_unique, key)
+                                         : hash_lookup(hkeys, hvals, hmask, key);
     out[i] = static_cast<int32_t>(r);
   }
 }
@@ -300,6 +319,24 @@ extern "C" int sqd_xsource(sqd_space_t s, uint64_t x, int lookup, int32_t* out, 
     cudaStream_t st = as_stream(stream);
     k_xsource<<<grid_for(s->states_size, 256, 8192), 256, 0, st>>>(
         s->states.ptr, s->n_unique, s->states_size, x, s->hkeys.ptr, s->hvals.ptr, s->hmask,
+        lookup == SQD_LOOKUP_BSEARCH ? SQD_LOOKUP_BSEARCH : SQD_LOOKUP_HASH, out);
+    SQD_CHECK_LAUNCH();
+  });
+}
+
+extern "C" int sqd_space_lookup(sqd_space_t s, const uint64_t* keys, int64_t n, int lookup,
+                                int32_t* out, void* stream) {
+  return guarded([&] {
+    SQD_REQUIRE(s != nullptr, "NULL space handle");
+    SQD_REQUIRE(n >= 0, "negative key count");
+    SQD_REQUIRE(n == 0 || (keys != nullptr && out != nullptr), "NULL argument");
+    SQD_REQUIRE(lookup == SQD_LOOKUP_HASH || lookup == SQD_LOOKUP_BSEARCH ||
+                    lookup == SQD_LOOKUP_AUTO,
+                "sqd_space_lookup takes SQD_LOOKUP_HASH, SQD_LOOKUP_BSEARCH or SQD_LOOKUP_AUTO");
+    if (n == 0) return;
+    cudaStream_t st = as_stream(stream);
+    k_lookup_keys<<<grid_for(n, 256, 8192), 256, 0, st>>>(
+        keys, n, s->fill_state, s->states.ptr, s->n_unique, s->hkeys.ptr, s->hvals.ptr, s->hmask,
         lookup == SQD_LOOKUP_BSEARCH ? SQD_LOOKUP_BSEARCH : SQD_LOOKUP_HASH, out);
     SQD_CHECK_LAUNCH();
   });

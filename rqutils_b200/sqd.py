@@ -128,6 +128,15 @@ class Subspace:
                   _lib.ptr(out), _lib.stream_ptr())
         return out
 
+    def lookup(self, keys, lookup='hash'):
+        """Sorted index of each key (int64 CUDA tensor of uint64 bit patterns), -1 when the
+        key is not a state of the subspace: int32 CUDA tensor."""
+        keys = keys.to(self.device, torch.int64).contiguous()
+        out = torch.empty(keys.shape[0], dtype=torch.int32, device=self.device)
+        _lib.call('sqd_space_lookup', self._handle, _lib.ptr(keys), keys.shape[0],
+                  _LOOKUPS[lookup], _lib.ptr(out), _lib.stream_ptr())
+        return out
+
 
 class SQDOperator:
     """The Hamiltonian projected on a subspace; callable as ``op(v) -> Hv``."""
@@ -343,19 +352,113 @@ def run_sqd(hamiltonian, states, states_size, options=None):
     return result
 
 
-def uniquify_states(states, states_size):
-    """uniquify_states (sqd.py:445-482) on binary [N, n] states: a ``Subspace``."""
-    return Subspace.from_bits(states, states_size)
+def _packed_rows(states_p):
+    """The reference's packed state rows (sqd.py:255: pad bit, then the qubits, big-endian;
+    uint8 [N, B]) as big-endian row values: (int64 CUDA tensor, B, fill-row mask).  Rows of 255
+    are the reference's fill rows; any other row with the pad bit set is rejected."""
+    _lib.require_cuda()
+    dev = torch.device('cuda', torch.cuda.current_device())
+    t = states_p if isinstance(states_p, torch.Tensor) else torch.as_tensor(np.asarray(states_p))
+    if t.dtype != torch.uint8 or t.dim() != 2:
+        raise ValueError('packed states must be a uint8 array of shape [N, B]')
+    b = t.shape[1]
+    if not 1 <= b <= 8:
+        raise ValueError('packed rows of 1 to 8 bytes (up to 63 qubits) are supported')
+    t = t.to(dev)
+    keys = torch.zeros(t.shape[0], dtype=torch.int64, device=dev)
+    for c in range(b):
+        keys = (keys << 8) | t[:, c].to(torch.int64)
+    fill = (t == 255).all(dim=1)
+    if bool(((t[:, 0] >= 128) & ~fill).any()):
+        raise ValueError('a packed state row has the pad bit set but is not a fill row of 255')
+    return keys, b, fill
 
 
-def get_xsource(xsignature, space, lookup='hash'):
-    """get_xsource (sqd.py:485-548) for a ``Subspace`` and one X mask (uint64 or labels'
-    packed bytes)."""
-    if isinstance(xsignature, (np.ndarray, list, tuple)):
-        from .paulis.symplectic import _unpack_masks
-        xsignature = int(_unpack_masks(np.asarray(xsignature, dtype=np.uint8)[None, :],
-                                       space.num_qubits, True)[0])
-    return space.xsource(int(xsignature), lookup)
+def _packed_x(xsignature, b):
+    x = np.asarray(xsignature, dtype=np.uint8).reshape(-1)
+    if x.shape[0] != b:
+        raise ValueError(f'xsignature has {x.shape[0]} bytes, the states {b}')
+    if x[0] >= 128:
+        raise ValueError('xsignature has the pad bit set')
+    return int.from_bytes(x.tobytes(), 'big')
+
+
+def uniquify_states(states_p, states_size, return_indices=False):
+    """uniquify_states (sqd.py:445-482) on the reference's packed rows (uint8 [N, B]): the sorted
+    unique rows followed by rows of 255 up to ``states_size`` (a uint8 CUDA tensor), and with
+    ``return_indices`` the input index of each kept row (its last occurrence, as the reference's
+    stable sort gives; -1 for fill rows).  Sorting and de-duplication run on the device
+    (``Subspace``); ``Subspace.from_bits`` takes binary states instead.  As in the reference, a
+    ``states_size`` below the number of unique rows keeps the first ``states_size`` of them."""
+    keys, b, fill = _packed_rows(states_p)
+    dev = keys.device
+    states_size = int(states_size)
+    real_idx = torch.nonzero(~fill).flatten()
+    real = keys[real_idx]
+    out = torch.full((states_size, b), 255, dtype=torch.uint8, device=dev)
+    idx = torch.full((states_size,), -1, dtype=torch.int32, device=dev)
+    n_u = 0
+    if real.numel():
+        space = Subspace.from_u64(real, 8 * b - 1)
+        uniq = space.states()
+        n_u = uniq.numel()
+        m = min(n_u, states_size)
+        for c in range(b):
+            out[:m, c] = ((uniq[:m] >> (8 * (b - 1 - c))) & 255).to(torch.uint8)
+        if return_indices:
+            pos = space.lookup(real).long()
+            last = torch.full((n_u,), -1, dtype=torch.int64, device=dev)
+            last.scatter_reduce_(0, pos, real_idx, reduce='amax')
+            idx[:m] = last[:m].to(torch.int32)
+    if return_indices and bool(fill.any()) and n_u < states_size:
+        idx[n_u] = int(torch.nonzero(fill).max())   # the rows of 255 sort last
+    return (out, idx) if return_indices else out
+
+
+def get_xsource(xsignature, states, sorted_input=True, lookup='hash'):
+    """get_xsource (sqd.py:485-548): int32 CUDA tensor, entry i the index of the row equal to
+    row i XOR x, or -1.
+
+    ``states`` is a ``Subspace`` (x: uint64 or packed bytes) or, as in the reference, packed rows
+    (uint8 [N, B], x: B packed bytes).  With ``sorted_input=True`` the rows must be sorted and
+    unique, optionally followed by fill rows of 255 (the output of ``uniquify_states``); the fill
+    rows get the values the reference's sort-based algorithm gives them.  With
+    ``sorted_input=False`` the rows may come in any order (sqd.py:515-516, 542-545) and indices
+    refer to the input order; duplicate rows and fill rows are rejected there, because the
+    reference's scatter then writes one position several times (its result is undefined)."""
+    if isinstance(states, Subspace):
+        if isinstance(xsignature, (np.ndarray, list, tuple)):
+            from .paulis.symplectic import _unpack_masks
+            xsignature = int(_unpack_masks(np.asarray(xsignature, dtype=np.uint8)[None, :],
+                                           states.num_qubits, True)[0])
+        return states.xsource(int(xsignature), lookup)
+    keys, b, fill = _packed_rows(states)
+    x = _packed_x(xsignature, b)
+    n = keys.shape[0]
+    dev = keys.device
+    if n == 0:
+        return torch.empty(0, dtype=torch.int32, device=dev)
+    nq = 8 * b - 1
+    if sorted_input:
+        n_real = int((~fill).sum())
+        ok = bool((~fill[:n_real]).all()) and bool(fill[n_real:].all()) and n_real > 0
+        ok = ok and bool((keys[1:n_real] > keys[:n_real - 1]).all())
+        if not ok:
+            raise ValueError('sorted_input=True needs sorted unique rows followed by fill rows '
+                             'of 255 (the output of uniquify_states); pass sorted_input=False')
+        return Subspace.from_u64(keys[:n_real], nq, states_size=n).xsource(x, lookup)
+    if bool(fill.any()):
+        raise ValueError('fill rows of 255 with sorted_input=False: the reference scatters them '
+                         'all to one position')
+    space = Subspace.from_u64(keys, nq)
+    if space.n_unique != n:
+        raise ValueError('duplicate rows with sorted_input=False: the reference scatters them '
+                         'to one position')
+    pos = space.lookup(keys).long()
+    inv = torch.empty(n, dtype=torch.int64, device=dev)
+    inv[pos] = torch.arange(n, dtype=torch.int64, device=dev)
+    src = space.lookup(keys ^ x, lookup).long()
+    return torch.where(src >= 0, inv[src.clamp(min=0)], torch.full_like(src, -1)).to(torch.int32)
 
 
 def get_diagonal(op, group):

@@ -183,3 +183,49 @@ def test_product_subspace_source_structure():
             ok_l = pl < nl and los[pl] == ((int(s) & int(lo_mask)) ^ xl)
             expect = ph * nl + pl if (ok_h and ok_l) else -1
             assert src[r] == expect
+
+
+def _uniquify_indices_literal(states_p, states_size):
+    """The index arithmetic of uniquify_states (sqd.py:457-481) transcribed step by step:
+    stable lexsort, is_unique over positions 1..N-1, cumsum(bincount(cumsum)), -1 past the
+    unique count."""
+    keys = tuple(states_p[:, b] for b in range(states_p.shape[1] - 1, -1, -1))
+    perm = np.lexsort(keys)
+    srt = states_p[perm]
+    is_unique = np.any(srt[1:] != srt[:-1], axis=1)
+    total_unique = int(is_unique.sum()) + 1
+    counts = np.bincount(np.cumsum(is_unique), minlength=states_size)[:states_size]
+    idx_unique = np.cumsum(counts)
+    idx_unique = np.where(np.arange(states_size) < total_unique, idx_unique, -1)
+    return np.where(idx_unique >= 0, perm[np.clip(idx_unique, 0, None)], -1)
+
+
+def test_uniquify_states_keeps_last_occurrence():
+    rng = np.random.default_rng(12)
+    bits = rng.integers(0, 2, size=(400, 7)).astype(np.uint8)     # many repeats of 128 strings
+    sp = OQ.pack_states(bits)
+    n_u = np.unique(sp, axis=0).shape[0]
+    for size in (n_u, n_u + 9, n_u - 5, 400):
+        rows, idx = OQ.uniquify_states(sp, size, return_indices=True)
+        assert (idx == _uniquify_indices_literal(sp, size)).all()
+        kept = idx >= 0
+        assert (rows[kept] == sp[idx[kept]]).all()
+        assert (rows[~kept] == 255).all()
+        # last occurrence: no later input row repeats a kept row
+        for i in np.flatnonzero(kept)[:40]:
+            later = sp[idx[i] + 1:]
+            assert not np.any(np.all(later == rows[i], axis=1))
+
+
+def test_get_xsource_unsorted_input_restatement():
+    rng = np.random.default_rng(13)
+    bits = np.unique(rng.integers(0, 2, size=(300, 10)).astype(np.uint8), axis=0)
+    sp = OQ.pack_states(bits)
+    perm = rng.permutation(sp.shape[0])
+    rows = sp[perm]
+    for x in (OQ.pack_states(rng.integers(0, 2, size=(1, 10)).astype(np.uint8))[0]
+              for _ in range(6)):
+        got = OQ.get_xsource_unsorted(x, rows)
+        table = {r.tobytes(): i for i, r in enumerate(rows)}
+        expect = [table.get(np.bitwise_xor(r, x).tobytes(), -1) for r in rows]
+        assert (got == np.array(expect)).all()
