@@ -16,6 +16,7 @@ sample).  ``--impl reference`` times only that CPU path.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                        [--workload c2|c1|c3|c5] [--cache 1,0|1,2|0,0] [--no-locg]
+                       [--precision fp64|fp32]
 """
 import argparse
 import json
@@ -52,6 +53,9 @@ def parse():
     ap.add_argument('--chunk', type=int, default=0, help='rows per block chunk with --lanes')
     ap.add_argument('--layout', default='csr', choices=['csr', 'product', 'product-csr'],
                     help='element layout with --lanes (the autotuner picks it otherwise)')
+    ap.add_argument('--precision', default='fp64', choices=['fp64', 'fp32'],
+                    help='vectors of the timed matvec: complex128 (default) or complex64 with '
+                         'FP32 elements and compensated sums (the bulk of the mixed solver)')
     return ap.parse_args()
 
 
@@ -81,10 +85,13 @@ def load_peaks():
     return 6650.0, 'fallback'
 
 
-def load_traffic(workload, cache, layout='csr'):
-    """DRAM traffic of one matvec (all its kernels) from the committed ncu summary."""
+def load_traffic(workload, cache, layout='csr', precision='fp64'):
+    """DRAM traffic of one matvec (all its kernels) from the committed ncu summary; FP32
+    vectors have their own summaries (suffix _fp32)."""
     names = [''] if layout == 'csr' else [f'_{layout}', '_product', '_product-csr']
-    paths = [os.path.join(ROOT, 'profiles', f'matvec_{workload}_cache{cache[0]}{cache[1]}{n}.md')
+    suffix = '' if precision == 'fp64' else '_' + precision
+    paths = [os.path.join(ROOT, 'profiles',
+                          f'matvec_{workload}_cache{cache[0]}{cache[1]}{n}{suffix}.md')
              for n in names]
     paths = [p for p in paths if os.path.exists(p)]
     if not paths:
@@ -290,7 +297,8 @@ def run_ours(args):
     j_groups = ham.num_groups
     nnz = op.nnz
 
-    v = torch.as_tensor(wl.start_vector(np.complex128), device=dev)
+    prec = 0 if args.precision == 'fp64' else 1
+    v = torch.as_tensor(wl.start_vector(np.complex128 if prec == 0 else np.complex64), device=dev)
     out = torch.empty_like(v)
     stream = torch.cuda.current_stream()
     for _ in range(max(3, args.warmup)):
@@ -317,7 +325,7 @@ def run_ours(args):
     value, t_max = replica_throughput(units, args.steps, t_local, dist)
     # kernels per matvec: CSR layout 1; product layout: transpose, low-half slabs, transpose,
     # two-half CSR tails (when there are any), high-half slabs
-    layout = op.get_layout(0) if cache == (1, 2) else 'csr'
+    layout = op.get_layout(prec) if cache == (1, 2) else 'csr'
     per_step = 1
     if layout in ('product', 'product-csr'):
         per_step = 5 if op.product_info()['pairs_mixed'] > 0 else 4
@@ -333,15 +341,17 @@ def run_ours(args):
     step_s = t_max / args.steps
 
     # roofline of the matvec kernel (algorithmic bytes per launch)
-    w_v, w_c, W = 16, 16, 1
+    w_v, w_c, W = v.element_size(), 16, 1
     bytes_alg = n_rows * (8 * W + 2 * w_v) + nnz * w_v + m_terms * (8 * W + w_c) + j_groups * 8 * W
     peak, peak_kind = load_peaks()
     achieved = bytes_alg / (t_local / args.steps) / 1e9
-    traffic = load_traffic(args.workload, cache, layout)
+    traffic = load_traffic(args.workload, cache, layout, args.precision)
     props = torch.cuda.get_device_properties(dev)
     sm_mhz = clocks['sm_mhz'] if clocks and clocks.get('sm_mhz') else 1965.0
-    issue = issue_bound(n_rows, m_terms, nnz, op.value_complex, props.multi_processor_count,
-                        sm_mhz, t_local / args.steps)
+    issue = None
+    if prec == 0:
+        issue = issue_bound(n_rows, m_terms, nnz, op.value_complex,
+                            props.multi_processor_count, sm_mhz, t_local / args.steps)
 
     extra = {}
     if not args.no_locg and rank == 0:
@@ -355,13 +365,15 @@ def run_ours(args):
             'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': step_s * 1e3,
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
-            'dtype': 'complex128 (f64 arithmetic)', 'data': 'synthetic (seeded generator)',
+            'dtype': ('complex128 (f64 arithmetic)' if prec == 0 else
+                      'complex64 (f32 products, compensated sums, f64 partials)'),
+            'data': 'synthetic (seeded generator)',
             'config': {**workload_config(wl, cache), 'parallelism': f'replicas x{world}',
                        'merged_terms': m_terms, 'x_groups': j_groups, 'stored_pairs': nnz,
                        'lanes_per_row': {'fp64': op.get_lanes(0), 'fp32': op.get_lanes(1)},
                        'layout': {'fp64': layout,
                                   'fp32': op.get_layout(1) if cache == (1, 2) else 'csr'},
-                       'kernels_per_matvec': per_step,
+                       'kernels_per_matvec': per_step, 'precision': args.precision,
                        'autotune': tuned,
                        'setup_s': setup_s},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
@@ -369,12 +381,13 @@ def run_ours(args):
                          'peak_kind': peak_kind,
                          'bytes_alg_per_launch': bytes_alg,
                          'formula': 'N(8W+2w_v) + P_valid w_v + M(8W+w_c) + J 8W, W=1, '
-                                    'w_v=16, w_c=16, P_valid = stored pairs',
-                         'timed': 'one whole FP64 matvec (all its kernels) per launch'},
+                                    f'w_v={w_v}, w_c=16, P_valid = stored pairs',
+                         'timed': f'one whole {args.precision.upper()} matvec (all its kernels) '
+                                  'per launch'},
             'issue_bound': issue,
             'e2e': {'value': e2e_value, 'unit': UNIT,
-                    'h2d_bytes_per_step': int(v.numel() * 16),
-                    'd2h_bytes_per_step': int(v.numel() * 16)},
+                    'h2d_bytes_per_step': int(v.numel() * v.element_size()),
+                    'd2h_bytes_per_step': int(v.numel() * v.element_size())},
             'gpu_launches': gpu_launches,
             'clocks': clocks,
         }

@@ -44,3 +44,8 @@ def test_issue_bound_estimate():
     assert b['cached_fp64_fma_floor_ms'] < 0.1 * b['timed_matvec_ms']
     assert bench.issue_bound(n, m, p, True, 148, 1965.0, 6.0e-3)['cached_fp64_fma_per_matvec'] \
         == 4 * p
+
+
+def test_fp32_traffic_uses_its_own_summaries():
+    assert bench.load_traffic('c2', (1, 2), 'product-csr', 'fp32') is None
+    assert bench.load_traffic('c2', (1, 2), 'product-csr', 'fp64') is not None
