@@ -628,12 +628,24 @@ void build_tail(sqd_op_s* op, cudaStream_t st) {
   const bool smem = build_tail_smem(op, len, st);
   if (L.pairs_m > kCompactTailMax * n) return;
   const int nca = op->value_complex ? 2 : 1;
-  if (!smem) {
-    L.mptr.alloc(n + 1, st);
-    exclusive_scan_i64(len.ptr, L.mptr.ptr, n, true, st);
-    L.mval.alloc(static_cast<size_t>(L.pairs_m) * nca, st);
+  // The copy is optional: without device memory for it the tails are read in place.
+  try {
+    if (!smem) {
+      L.mptr.alloc(n + 1, st);
+      L.mval.alloc(static_cast<size_t>(L.pairs_m) * nca, st);
+    }
+    L.mcol.alloc(static_cast<size_t>(L.pairs_m), st);
+  } catch (const Error& e) {
+    if (e.status != SQD_ERR_MEMORY) throw;
+    (void)cudaGetLastError();  // the failed pool allocation
+    if (!smem) {
+      L.mptr = DevBuf<int64_t>();
+      L.mval = DevBuf<double>();
+    }
+    L.mcol = DevBuf<uint32_t>();
+    return;
   }
-  L.mcol.alloc(static_cast<size_t>(L.pairs_m), st);
+  if (!smem) exclusive_scan_i64(len.ptr, L.mptr.ptr, n, true, st);
   const unsigned G = grid_for(n, 256, 16384);
   if (nca == 2)
     k_tail_fill<2><<<G, 256, 0, st>>>(op->row_ptr.ptr, op->cols.ptr, op->values.ptr, L.ho.ptr,
