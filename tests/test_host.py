@@ -71,3 +71,25 @@ def test_every_package_module_imports():
     assert 'rqutils_b200.autotune' in names
     for name in names:
         importlib.import_module(name)
+
+
+@pytest.mark.parametrize('norb', [3, 5])
+def test_jw_structure_map_reproduces_the_jw_hamiltonian(norb):
+    """The batched workload's shortcut (a fixed sparse map from the independent integrals to the
+    Pauli coefficients) gives the same Pauli sum as the direct Jordan-Wigner construction."""
+    from rqutils_b200 import workloads as W
+    rng = np.random.default_rng(40 + norb)
+    h1, h2 = W.random_integrals(norb, rng)
+    st = W.JWStructure(norb)
+
+    def as_dict(x, z, c):
+        d = {}
+        for xi, zi, ci in zip(np.asarray(x, np.uint64), np.asarray(z, np.uint64), np.asarray(c)):
+            d[(int(xi), int(zi))] = d.get((int(xi), int(zi)), 0.0) + complex(ci)
+        return {k: v for k, v in d.items() if abs(v) > 1e-12}
+
+    direct = as_dict(*W.jw_hamiltonian(h1, h2))
+    mapped = as_dict(*st.hamiltonian(h1, h2))
+    assert direct.keys() == mapped.keys()
+    scale = max(abs(v) for v in direct.values())
+    assert max(abs(direct[k] - mapped[k]) for k in direct) <= 1e-13 * scale
