@@ -374,8 +374,12 @@ def _packed_rows(states_p):
     return keys, b, fill
 
 
+def _host_array(a):
+    return a.detach().cpu().numpy() if isinstance(a, torch.Tensor) else a
+
+
 def _packed_x(xsignature, b):
-    x = np.asarray(xsignature, dtype=np.uint8).reshape(-1)
+    x = np.asarray(_host_array(xsignature), dtype=np.uint8).reshape(-1)
     if x.shape[0] != b:
         raise ValueError(f'xsignature has {x.shape[0]} bytes, the states {b}')
     if x[0] >= 128:
@@ -426,6 +430,7 @@ def get_xsource(xsignature, states, sorted_input=True, lookup='hash'):
     ``sorted_input=False`` the rows may come in any order (sqd.py:515-516, 542-545) and indices
     refer to the input order; duplicate rows and fill rows are rejected there, because the
     reference's scatter then writes one position several times (its result is undefined)."""
+    xsignature = _host_array(xsignature)
     if isinstance(states, Subspace):
         if isinstance(xsignature, (np.ndarray, list, tuple)):
             from .paulis.symplectic import _unpack_masks

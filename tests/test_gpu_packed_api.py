@@ -47,6 +47,10 @@ def test_get_xsource_packed_sorted_rows_with_fill(lookup):
     for x in ham.x:
         got = rq.get_xsource(x, sp, lookup=lookup).cpu().numpy()
         assert (got == OQ.get_xsource(x, sp)).all()
+    # device tensors in, as a caller holding them on the GPU would pass them
+    x = ham.x[1]
+    got = rq.get_xsource(torch.as_tensor(x).cuda(), torch.as_tensor(sp).cuda(), lookup=lookup)
+    assert (got.cpu().numpy() == OQ.get_xsource(x, sp)).all()
 
 
 def test_get_xsource_packed_unsorted_rows():
