@@ -80,7 +80,8 @@ struct ProductLayout {
   sqd::DevBuf<int64_t> ho, lo;       // [nh + 1], [nl + 1]
   sqd::DevBuf<uint32_t> hsrc, lsrc;  // [th], [tl]
   sqd::DevBuf<double> vh, vl;        // FP64 elements (x2 interleaved when complex)
-  sqd::DevBuf<float> vh32, vl32;     // FP32 copies
+  sqd::DevBuf<float> vh32, vl32;     // FP32 copies (64-wide panels when wide32)
+  int wide32 = 0;                    // both halves even: FP32 slabs read two positions per lane
   sqd::DevBuf<double> vt, tt, t;     // per-matvec scratch: transposed input, L and M partials
   // Compact copies of the row tails (the M pairs of each row, contiguous: mptr, mval) with the
   // sources in one or both of two forms.  Shared memory (tail_slots > 0), when every slab's M

@@ -200,6 +200,24 @@ __global__ void k_to_float32(const double* __restrict__ in, float* __restrict__ 
     out[i] = static_cast<float>(in[i]);
 }
 
+// FP32 copy of a slab in 64-wide panels: out[((b / 64) * total_k + k) * 64 + b % 64] =
+// in[panel_index(k, b, total_k)] for b < B, zero in the padding of the last panel.
+template <int NCA>
+__global__ void k_float_panels64(const double* __restrict__ in, int64_t total_k, int64_t B,
+                                 float* __restrict__ out) {
+  const int64_t n = ((B + 63) / 64) * total_k * 64;
+  for (int64_t q = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; q < n;
+       q += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t rest = q >> 6, pos = q & 63;   // rest = panel * total_k + k
+    const int64_t p = rest / total_k, k = rest - p * total_k;
+    const int64_t b = p * 64 + pos;
+    const int64_t src = b < B ? panel_index(k, b, total_k) : 0;
+#pragma unroll
+    for (int t = 0; t < NCA; ++t)
+      out[NCA * q + t] = b < B ? static_cast<float>(in[NCA * src + t]) : 0.0f;
+  }
+}
+
 // out[c][r] = in[r][c] for an rows x cols matrix of elements E (32 x 32 tiles, 256 threads).
 template <typename E>
 __global__ void __launch_bounds__(256)
@@ -272,6 +290,106 @@ k_slab(int64_t A, int64_t B, int64_t total_k, int64_t a_tiles, const int64_t* __
     }
     if constexpr (FINAL) st_elem<R, NCV>(out, a * B + b, cx_make<R>(acc.re.value(), acc.im.value()));
     else acc.store_partial(out_part, a * B + b);
+  }
+}
+
+// FP32 slabs in 64-wide panels: a lane owns two adjacent positions b, b + 1, so one 16-byte
+// (complex64) or 8-byte (float) load reads both amplitudes and one 8- or 16-byte load both
+// elements; four entries per step.  Same sums per position as k_slab (FMA chains of four
+// products into the compensated sums).  VEC: x and out allow the paired vector accesses
+// (source offsets and B even, pointers aligned), else each position is read on its own.
+template <typename R, int NCA>
+__device__ __forceinline__ void pair_elem(const R* p, Cx<R>& e0, Cx<R>& e1) {
+  if constexpr (NCA == 2) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    e0 = cx_make<R>(v.x, v.y);
+    e1 = cx_make<R>(v.z, v.w);
+  } else {
+    const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+    e0 = cx_make<R>(v.x, R(0));
+    e1 = cx_make<R>(v.y, R(0));
+  }
+}
+
+template <typename R, int NCV, bool VEC>
+__device__ __forceinline__ void pair_vec(const R* x, int64_t i, Cx<R>& v0, Cx<R>& v1) {
+  if constexpr (VEC && NCV == 2) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(x + 2 * i));
+    v0 = cx_make<R>(v.x, v.y);
+    v1 = cx_make<R>(v.z, v.w);
+  } else if constexpr (VEC) {
+    const float2 v = __ldg(reinterpret_cast<const float2*>(x + i));
+    v0 = cx_make<R>(v.x, R(0));
+    v1 = cx_make<R>(v.y, R(0));
+  } else {
+    v0 = ld_elem<R, NCV>(x, i);
+    v1 = ld_elem<R, NCV>(x, i + 1);
+  }
+}
+
+template <typename R, int NCV, int NCA, bool FINAL, bool HAS_M, bool VEC>
+__global__ void __launch_bounds__(256)
+k_slab2(int64_t A, int64_t B, int64_t total_k, int64_t a_tiles, const int64_t* __restrict__ off,
+        const uint32_t* __restrict__ src, const R* __restrict__ V, const R* __restrict__ x,
+        const double* __restrict__ part_t, const double* __restrict__ part_m, R* __restrict__ out,
+        double* __restrict__ out_part) {
+  static_assert(sizeof(R) == 4, "two positions per lane: FP32 slabs");
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t panels = (B + 63) >> 6;
+  for (int64_t blk = blockIdx.x; blk < panels * a_tiles; blk += gridDim.x) {
+    const int64_t p = blk / a_tiles;
+    const int64_t a = (blk - p * a_tiles) * 8 + warp;
+    const int64_t b = p * 64 + 2 * lane;  // positions b and b + 1 (B is even)
+    if (a >= A || b >= B) continue;
+    CAcc<R, NCV, NCA> acc0, acc1;
+    if constexpr (FINAL) {
+      acc0.add_partial(part_t, a * B + b);
+      acc1.add_partial(part_t, a * B + b + 1);
+      if constexpr (HAS_M) {
+        acc0.add_partial(part_m, a * B + b);
+        acc1.add_partial(part_m, a * B + b + 1);
+      }
+    }
+    const int64_t k1 = __ldg(off + a + 1);
+    int64_t k = __ldg(off + a);
+    const R* vp = V + ((p * total_k + k) * 64 + 2 * lane) * NCA;
+    for (; k + 3 < k1; k += 4) {
+      uint32_t si[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) si[u] = __ldg(src + k + u);
+      Cx<R> m0[4], m1[4], x0[4], x1[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        pair_elem<R, NCA>(vp + 64 * NCA * u, m0[u], m1[u]);
+        pair_vec<R, NCV, VEC>(x, int64_t(si[u]) + b, x0[u], x1[u]);
+      }
+      acc0.add4(m0, x0);
+      acc1.add4(m1, x1);
+      vp += 4 * 64 * NCA;
+    }
+    for (; k < k1; ++k) {
+      Cx<R> m0, m1, x0, x1;
+      pair_elem<R, NCA>(vp, m0, m1);
+      pair_vec<R, NCV, VEC>(x, int64_t(__ldg(src + k)) + b, x0, x1);
+      acc0.add(m0, x0);
+      acc1.add(m1, x1);
+      vp += 64 * NCA;
+    }
+    if constexpr (FINAL) {
+      if constexpr (VEC && NCV == 2) {
+        reinterpret_cast<float4*>(out)[(a * B + b) >> 1] =
+            make_float4(acc0.re.value(), acc0.im.value(), acc1.re.value(), acc1.im.value());
+      } else if constexpr (VEC) {
+        reinterpret_cast<float2*>(out)[(a * B + b) >> 1] =
+            make_float2(acc0.re.value(), acc1.re.value());
+      } else {
+        st_elem<R, NCV>(out, a * B + b, cx_make<R>(acc0.re.value(), acc0.im.value()));
+        st_elem<R, NCV>(out, a * B + b + 1, cx_make<R>(acc1.re.value(), acc1.im.value()));
+      }
+    } else {
+      acc0.store_partial(out_part, a * B + b);
+      acc1.store_partial(out_part, a * B + b + 1);
+    }
   }
 }
 
@@ -498,11 +616,25 @@ unsigned capped_grid(int64_t blocks) {
   return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(blocks, INT_MAX)));
 }
 
+// wide: FP32 slabs in 64-wide panels (k_slab2); vec: x and out allow its paired accesses.
 template <typename R, int NCV, int NCA, bool FINAL, bool HAS_M>
 void launch_slab(int64_t A, int64_t B, int64_t total_k, const int64_t* off, const uint32_t* src,
                  const R* V, const R* x, const double* part_t, const double* part_m, R* out,
-                 double* out_part, cudaStream_t st) {
+                 double* out_part, cudaStream_t st, bool wide = false, bool vec = false) {
   if (A == 0 || B == 0) return;
+  if constexpr (sizeof(R) == 4) {
+    if (wide) {
+      const int64_t a_tiles = (A + 7) / 8, panels = (B + 63) / 64;
+      if (vec)
+        k_slab2<R, NCV, NCA, FINAL, HAS_M, true><<<capped_grid(a_tiles * panels), 256, 0, st>>>(
+            A, B, total_k, a_tiles, off, src, V, x, part_t, part_m, out, out_part);
+      else
+        k_slab2<R, NCV, NCA, FINAL, HAS_M, false><<<capped_grid(a_tiles * panels), 256, 0, st>>>(
+            A, B, total_k, a_tiles, off, src, V, x, part_t, part_m, out, out_part);
+      SQD_CHECK_LAUNCH();
+      return;
+    }
+  }
   const int64_t a_tiles = (A + 7) / 8, panels = (B + 31) / 32;
   // With at most two waves of warps (64 per SM) too few warps hide the latency of each step's
   // source-offset load, which the gathers wait on, so it is prefetched one step ahead (C2:
@@ -549,6 +681,29 @@ void to_float(const DevBuf<double>& in, DevBuf<float>& out, cudaStream_t st) {
   k_to_float32<<<grid_for(static_cast<int64_t>(in.count), 256, 16384), 256, 0, st>>>(
       in.ptr, out.ptr, static_cast<int64_t>(in.count));
   SQD_CHECK_LAUNCH();
+}
+
+// FP32 copies of both slab sets: 64-wide panels when wide32, else the FP64 layout.
+void slabs_to_float(sqd_op_s* op, cudaStream_t st) {
+  ProductLayout& L = op->prod;
+  if (!L.wide32) {
+    to_float(L.vh, L.vh32, st);
+    to_float(L.vl, L.vl32, st);
+    return;
+  }
+  const int nca = op->value_complex ? 2 : 1;
+  auto conv = [&](const DevBuf<double>& in, int64_t total_k, int64_t B, DevBuf<float>& out) {
+    const int64_t n = ((B + 63) / 64) * total_k * 64;
+    out.alloc(static_cast<size_t>(std::max<int64_t>(n, 1)) * nca, st);
+    const unsigned G = grid_for(std::max<int64_t>(n, 1), 256, 16384);
+    if (nca == 2)
+      k_float_panels64<2><<<G, 256, 0, st>>>(in.ptr, total_k, B, out.ptr);
+    else
+      k_float_panels64<1><<<G, 256, 0, st>>>(in.ptr, total_k, B, out.ptr);
+    SQD_CHECK_LAUNCH();
+  };
+  conv(L.vh, L.th, L.nl, L.vh32);
+  conv(L.vl, L.tl, L.nh, L.vl32);
 }
 
 // A row tail read in place is a short segment of the row's long pair list (C3-like subspaces:
@@ -996,6 +1151,7 @@ void op_product_build(sqd_op_s* op, cudaStream_t st) {
   ProductLayout L;
   L.nh = nh;
   L.nl = nl;
+  L.wide32 = (nh % 2 == 0 && nl % 2 == 0) ? 1 : 0;
   DevBuf<unsigned long long> bad;
   bad.alloc(1, st);
   SQD_CUDA(cudaMemsetAsync(bad.ptr, 0, sizeof(unsigned long long), st));
@@ -1060,8 +1216,7 @@ void op_product_build(sqd_op_s* op, cudaStream_t st) {
   }
   build_tail(op, st);
   if (op->values32.ptr && op->layout[1] != SQD_LAYOUT_CSR) {
-    to_float(op->prod.vh, op->prod.vh32, st);
-    to_float(op->prod.vl, op->prod.vl32, st);
+    slabs_to_float(op, st);
     if (op->prod.mval.ptr) to_float(op->prod.mval, op->prod.mval32, st);
   }
   op->prod.built = 1;
@@ -1074,16 +1229,14 @@ void op_product_values(sqd_op_s* op, cudaStream_t st) {
   extract(op, st, 0, nullptr);
   refill_tail(op, st);
   if (op->prod.vh32.ptr) {
-    to_float(op->prod.vh, op->prod.vh32, st);
-    to_float(op->prod.vl, op->prod.vl32, st);
+    slabs_to_float(op, st);
     if (op->prod.mval.ptr) to_float(op->prod.mval, op->prod.mval32, st);
   }
 }
 
 void op_product_values32(sqd_op_s* op, cudaStream_t st) {
   if (!op->prod.built || op->prod.vh32.ptr) return;
-  to_float(op->prod.vh, op->prod.vh32, st);
-  to_float(op->prod.vl, op->prod.vl32, st);
+  slabs_to_float(op, st);
   if (op->prod.mval.ptr) to_float(op->prod.mval, op->prod.mval32, st);
 }
 
@@ -1114,11 +1267,17 @@ void op_product_matvec(sqd_op_s* op, const void* v, void* out, int dtype, cudaSt
       VC = op->values32.ptr;
     }
     R* vt = reinterpret_cast<R*>(L.vt.ptr);
+    // FP32 slabs in 64-wide panels (both halves even): paired accesses to the library's own
+    // buffers always, to v and Hv when their addresses allow
+    const bool wide = sizeof(R) == 4 && L.wide32;
+    const uintptr_t pair_bytes = 2 * NCV * sizeof(R);
+    const bool vec_io = reinterpret_cast<uintptr_t>(vin) % pair_bytes == 0 &&
+                        reinterpret_cast<uintptr_t>(vout) % pair_bytes == 0;
     // 1. vT[l][h] = v[h][l]
     launch_transpose<E>(vin, vt, nh, nl, st);
     // 2. L part: t2[l][h]
     launch_slab<R, NCV, NCA, false, false>(nl, nh, L.tl, L.lo.ptr, L.lsrc.ptr, VL, vt, nullptr,
-                                           nullptr, nullptr, L.tt.ptr, st);
+                                           nullptr, nullptr, L.tt.ptr, st, wide, true);
     // 3. t2 back in row order, into the vT buffer
     launch_transpose<ED>(L.tt.ptr, L.vt.ptr, nl, nh, st);
     // 4. M part: t3[r]
@@ -1145,10 +1304,10 @@ void op_product_matvec(sqd_op_s* op, const void* v, void* out, int dtype, cudaSt
       }
       // 5. H part plus both partials
       launch_slab<R, NCV, NCA, true, true>(nh, nl, L.th, L.ho.ptr, L.hsrc.ptr, VH, vin, L.vt.ptr,
-                                           L.t.ptr, vout, nullptr, st);
+                                           L.t.ptr, vout, nullptr, st, wide, vec_io);
     } else {
       launch_slab<R, NCV, NCA, true, false>(nh, nl, L.th, L.ho.ptr, L.hsrc.ptr, VH, vin,
-                                            L.vt.ptr, nullptr, vout, nullptr, st);
+                                            L.vt.ptr, nullptr, vout, nullptr, st, wide, vec_io);
     }
   });
 }

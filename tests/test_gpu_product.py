@@ -266,3 +266,27 @@ def test_product_csr_tail_forms(seed, short):
                     op.set_lanes(prec, lanes)
                     op.set_chunk(prec, chunk)
                     assert rel(op.matvec(v.to(dt)).cpu().numpy(), ref) < tol
+
+
+@pytest.mark.parametrize('dtype', [torch.complex64, torch.float32])
+def test_fp32_slabs_with_unaligned_vectors(dtype):
+    """FP32 slabs of even-sized halves read two positions per lane with paired vector loads;
+    v and Hv that start off that alignment (views one element into a buffer) take the
+    element-wise path, with the same sums bit for bit."""
+    wl = _jw_small()
+    n = wl.num_qubits
+    ham = rq.PauliSumXZ.from_xz(wl.x, wl.z, wl.coeffs, n, force_real=True, padded=True)
+    op = rq.SQDOperator(ham, rq.Subspace.from_u64(wl.states, n), cache_strategy=(1, 2))
+    op.set_layout(1, 'product')
+    v = _vector(op.size, dtype, seed=8)
+    ref = _oracle_hv(wl.x, wl.z, wl.coeffs, wl.states, n, v.cpu().numpy(), True)
+    aligned = op.matvec(v)
+    assert rel(aligned.cpu().numpy(), ref) < MATVEC32_RTOL
+    vbuf = torch.zeros(op.size + 1, dtype=dtype, device='cuda')
+    vbuf[1:] = v
+    obuf = torch.zeros(op.size + 1, dtype=dtype, device='cuda')
+    op.matvec(vbuf[1:], obuf[1:])
+    assert torch.equal(obuf[1:], aligned)
+    out = torch.zeros_like(v)
+    op.matvec(vbuf[1:], out)                       # only the input off the pairing
+    assert torch.equal(out, aligned)
