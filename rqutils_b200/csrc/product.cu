@@ -24,13 +24,15 @@
 // same panel-major order, VH(k, l) at ((l / 32) * KH + k) * 32 + l % 32 (KH = entries of all
 // slabs), so the element stream of a panel pass is one contiguous sweep.  Source indices are
 // kept premultiplied (h' * nl, l' * nh).  At 48 qubits the FP64 passes stream their elements
-// at ~5 TB/s while L2 serves one amplitude per entry (~19 TB/s); FP32 passes are bound by the
-// latency of their index -> amplitude chains.
+// at ~5 TB/s while L2 serves one amplitude per entry (~19 TB/s).  The FP32 copies of the slabs
+// of even-sized halves use 64-wide panels, read by k_slab2 with two adjacent positions per
+// lane (paired 16-byte amplitude loads).
 // Step 4: when all M source slabs of every slab fit in shared memory together (small slabs,
 // e.g. 512 strings per half), k_tail_smem stages them per block and gathers from shared
 // memory through 16-bit indices of a compact copy of the row tails; otherwise (and under
 // SQD_LAYOUT_PRODUCT_CSR) the CSR kernel runs over the row tails, gathering from global
-// memory.
+// memory: from a contiguous copy of the tails (row offsets, elements, source rows) when they
+// average at most kCompactTailMax pairs per row, else inside the rows' pair lists.
 // FP32 vectors keep the compensated accumulation in every part and pass partials in FP64, so
 // the result is rounded once.  The elements are the same numbers as in the CSR arrays; only
 // the summation order of a row changes (L and M pairs before H pairs).
