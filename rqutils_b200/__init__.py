@@ -9,7 +9,9 @@ from .sqd import (SQDOptions, SQDOperator, Subspace, sqd, run_sqd, hproj, uniqui
                   get_xsource, get_diagonal)
 from .ground_locg import ground_locg
 
-_lib.load()
+# The shared library is mapped by the first call that needs it (``_lib.load()``, which raises
+# ImportError when the library is missing), so importing the package for its pure-Python parts
+# (the seeded workload generators, the option types) maps no native code.
 
 __all__ = ['PauliSumXZ', 'SQDOptions', 'SQDOperator', 'Subspace', 'sqd', 'run_sqd', 'hproj',
            'uniquify_states', 'get_xsource', 'get_diagonal', 'ground_locg']
