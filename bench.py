@@ -1,8 +1,10 @@
 """Benchmark of the SQD hot path on B200.
 
-Default workload (one GPU): the 32-qubit Jordan-Wigner molecular Hamiltonian (16 spatial
-orbitals, h1 ~ N(0,1)/16, h2 ~ N(0,0.1) with 8-fold symmetry, seed 0) on the 512 x 512
-alpha/beta product subspace of 4-electron strings (D = 262,144), complex128 vectors.
+Default workload (one GPU): the 48-qubit Jordan-Wigner molecular Hamiltonian (24 spatial
+orbitals, h1 ~ N(0,1)/16, h2 ~ N(0,0.1) with 8-fold symmetry, seed 0, 485,281 merged terms) on
+the 4096 x 4096 alpha/beta product subspace of 6-electron strings (D = 16,777,216), complex128
+vectors: the mixed-precision single-instance configuration.  ``--workload c2`` selects the
+32-qubit, 16-orbital construction on 512 x 512 4-electron strings (D = 262,144).
 
 A step is one Pauli-sum matvec Hv over the whole subspace (the inner kernel of LOCG).  ``value``
 is row.terms/s = (rows x merged terms) / step time, summed over ranks (replicas, weak scaling),
@@ -11,11 +13,12 @@ step's input vector copied from pinned host memory and its result copied back in
 timed region (copies of neighbouring steps overlap the matvec on separate streams).
 Beside it: the roofline of the matvec (its kernels together), the LOCG time-to-E0 (FP64 and
 mixed precision),
-and the CPU baseline (the reference's default matvec algorithm on the host cores, on a row
-sample).  ``--impl reference`` times only that CPU path.
+and the CPU baseline (the reference's default matvec algorithm on the host cores, on a fixed
+seeded row sample).  ``--impl reference`` times only that CPU path, on the same row sample, so
+the two CPU figures measure the same work.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                       [--workload c2|c1|c3|c5] [--cache 1,0|1,2|0,0] [--no-locg]
+                       [--workload c3|c2|c1|c5|c4] [--cache 1,0|1,2|0,0] [--no-locg]
                        [--precision fp64|fp32]
 """
 import argparse
@@ -42,13 +45,14 @@ def parse():
     ap.add_argument('--steps', type=int, default=20)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--workload', default='c2', choices=['c1', 'c2', 'c3', 'c4', 'c5', 'c3_small'])
+    ap.add_argument('--workload', default='c3', choices=['c1', 'c2', 'c3', 'c4', 'c5', 'c3_small'])
     ap.add_argument('--cache', default='1,2')
     ap.add_argument('--no-locg', action='store_true')
     ap.add_argument('--no-cpu', action='store_true')
     ap.add_argument('--no-graph', action='store_true',
                     help='LOCG without CUDA graphs (so a profiler sees every pass kernel)')
-    ap.add_argument('--cpu-rows', type=int, default=0, help='CPU sample rows (0 = auto)')
+    ap.add_argument('--cpu-rows', type=int, default=0,
+                    help='CPU sample rows (0 = the workload\'s fixed sample)')
     ap.add_argument('--lanes', type=int, default=0, help='lanes per row (0 = autotune)')
     ap.add_argument('--chunk', type=int, default=0, help='rows per block chunk with --lanes')
     ap.add_argument('--layout', default='csr', choices=['csr', 'product', 'product-csr'],
@@ -85,9 +89,25 @@ def load_peaks():
     return 6650.0, 'fallback'
 
 
+def kernel_sources_digest():
+    """SHA-256 over the CUDA sources (name and bytes, sorted by name): identifies the kernels
+    a profile summary was captured on."""
+    import hashlib
+    csrc = os.path.join(ROOT, 'rqutils_b200', 'csrc')
+    h = hashlib.sha256()
+    for name in sorted(os.listdir(csrc)):
+        if name.endswith(('.cu', '.cuh', '.h')):
+            h.update(name.encode())
+            with open(os.path.join(csrc, name), 'rb') as f:
+                h.update(f.read())
+    return h.hexdigest()
+
+
 def load_traffic(workload, cache, layout='csr', precision='fp64'):
-    """DRAM traffic of one matvec (all its kernels) from the committed ncu summary; FP32
-    vectors have their own summaries (suffix _fp32)."""
+    """DRAM traffic of one matvec (all its kernels) from the committed ncu summary of this
+    workload, layout and precision (FP32 vectors: suffix _fp32).  Used only when the summary's
+    ``kernel_sources_sha256`` equals the digest of the current sources; otherwise (kernels
+    changed since the capture) the traffic is reported as unknown.  Returns (bytes, note)."""
     names = [''] if layout == 'csr' else [f'_{layout}', '_product', '_product-csr']
     suffix = '' if precision == 'fp64' else '_' + precision
     paths = [os.path.join(ROOT, 'profiles',
@@ -95,12 +115,20 @@ def load_traffic(workload, cache, layout='csr', precision='fp64'):
              for n in names]
     paths = [p for p in paths if os.path.exists(p)]
     if not paths:
-        return None
-    path = paths[0]
-    for line in open(path):
-        if line.startswith('traffic_bytes_per_launch:'):
-            return float(line.split(':', 1)[1])
-    return None
+        return None, 'no ncu summary for this workload/layout'
+    fields = {}
+    with open(paths[0]) as f:
+        for line in f:
+            if ':' in line and line.split(':', 1)[0].strip() in (
+                    'traffic_bytes_per_launch', 'kernel_sources_sha256'):
+                k, v = line.split(':', 1)
+                fields[k.strip()] = v.strip()
+    rel = os.path.relpath(paths[0], ROOT)
+    if fields.get('kernel_sources_sha256') != kernel_sources_digest():
+        return None, f'{rel} was captured on other kernel sources'
+    if 'traffic_bytes_per_launch' not in fields:
+        return None, f'{rel} has no traffic line'
+    return float(fields['traffic_bytes_per_launch']), f'ncu capture in {rel}'
 
 
 class ClockSampler:
@@ -203,44 +231,56 @@ def barrier(dist):
         dist.barrier()
 
 
-def cpu_baseline(wl, budget_s=20.0, rows=0):
-    """The reference's default matvec on the host cores over a bounded row sample."""
+# Rows of the CPU sample per workload: about 1-3 s of host work per step on 16 cores.  The
+# cpu_baseline leg and the --impl reference arm time the same seeded sample.
+CPU_SAMPLE_ROWS = {'c1': 2000, 'c2': 32768, 'c3': 2048, 'c3_small': 8192, 'c5': 65536}
+
+
+def cpu_sample(wl, rows=0):
+    n = wl.states.shape[0]
+    rows = rows or CPU_SAMPLE_ROWS.get(wl.name, 16384)
+    rows = min(rows, n)
+    rng = np.random.default_rng(1)
+    return np.sort(rng.choice(n, size=rows, replace=False))
+
+
+def cpu_sample_desc(sample, n, m, extra=''):
+    return (f'{sample.shape[0]} of {n} rows (seeded uniform sample, rng 1), all {m} merged '
+            f'terms, one matvec per step{extra}; NumPy restatement of apply_h_x_cached + '
+            'get_diagonal (sqd.py:603-709) over a spawn process pool on every host core')
+
+
+def cpu_baseline(wl, rows=0):
+    """The reference's default matvec on the host cores over the workload's fixed row sample
+    (one warm-up step, one timed step)."""
     from oracle.cpu_baseline import CpuMatvecSample
     n = wl.states.shape[0]
-    rng = np.random.default_rng(1)
-    if rows <= 0:
-        rows = min(n, 16384)
-    sample = np.sort(rng.choice(n, size=min(rows, n), replace=False))
+    sample = cpu_sample(wl, rows)
     cpu = CpuMatvecSample(wl.x, wl.z, wl.coeffs, wl.states, sample)
     v = wl.start_vector(np.complex128)
     t1 = cpu.time(v, reps=1)
-    # grow the sample to fill about budget_s of CPU work
-    if rows < n and t1 < budget_s / 4:
-        scale = min(n / rows, max(1.0, budget_s / 2 / max(t1, 1e-3)))
-        new_rows = int(min(n, rows * scale))
-        cpu.close()
-        sample = np.sort(rng.choice(n, size=new_rows, replace=False))
-        cpu = CpuMatvecSample(wl.x, wl.z, wl.coeffs, wl.states, sample)
-        t1 = cpu.time(v, reps=1)
     m = cpu.num_terms
     cpu.close()
-    val = sample.shape[0] * m / t1
-    return {'value': val, 'unit': UNIT, 'cores': cpu.nproc, 'kind': 'port',
-            'sample': f'{sample.shape[0]} of {n} rows, all {m} merged terms, one matvec '
-                      f'({t1:.1f} s), NumPy restatement of apply_h_x_cached + get_diagonal '
-                      f'over a spawn process pool'}
+    return {'value': sample.shape[0] * m / t1, 'unit': UNIT, 'cores': cpu.nproc,
+            'kind': 'port', 'sample': cpu_sample_desc(sample, n, m, f' ({t1:.2f} s)')}
 
 
 def run_reference(args):
+    """The reference arm: the oracle port of the reference's default matvec (the reference
+    itself needs JAX, absent from this image) on every host core, on the same seeded row
+    sample as the cpu_baseline leg.  Maps no library of this repository."""
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
+        return
+    if args.workload == 'c4':
+        print(json.dumps({'impl': 'reference', 'unavailable':
+                          'c4 is a batched-solver workload; the CPU port times matvecs only'}),
+              flush=True)
         return
     wl = make_workload(args.workload)
     from oracle.cpu_baseline import CpuMatvecSample
     n = wl.states.shape[0]
-    rng = np.random.default_rng(1)
-    rows = args.cpu_rows or min(n, 16384)
-    sample = np.sort(rng.choice(n, size=rows, replace=False))
+    sample = cpu_sample(wl, args.cpu_rows)
     cpu = CpuMatvecSample(wl.x, wl.z, wl.coeffs, wl.states, sample)
     v = wl.start_vector(np.complex128)
     for _ in range(max(0, args.warmup)):
@@ -250,17 +290,14 @@ def run_reference(args):
         cpu.matvec(v)
     dt = (time.perf_counter() - t0) / max(1, args.steps)
     cpu.close()
-    val = rows * cpu.num_terms / dt
-    sample_desc = (f'{rows} of {n} rows per step, all {cpu.num_terms} merged terms, NumPy '
-                   'restatement of apply_h_x_cached + get_diagonal (sqd.py:603-709) over a '
-                   'spawn process pool')
+    val = sample.shape[0] * cpu.num_terms / dt
     line = {'impl': 'reference', 'metric': METRIC, 'value': val, 'unit': UNIT,
             'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
             'ms_per_step': dt * 1e3, 'higher_is_better': True, 'scaling': 'weak',
-            'vs_baseline': None, 'dtype': 'complex128', 'data': 'synthetic',
+            'vs_baseline': None, 'dtype': 'complex128 (f64 arithmetic)', 'data': 'synthetic',
             'config': workload_config(wl, (1, 0)),
             'cpu_baseline': {'value': val, 'unit': UNIT, 'cores': cpu.nproc, 'kind': 'port',
-                             'sample': sample_desc},
+                             'sample': cpu_sample_desc(sample, n, cpu.num_terms)},
             'e2e': {'value': val, 'unit': UNIT, 'h2d_bytes_per_step': 0,
                     'd2h_bytes_per_step': 0}}
     print(json.dumps(line), flush=True)
@@ -345,7 +382,10 @@ def run_ours(args):
     bytes_alg = n_rows * (8 * W + 2 * w_v) + nnz * w_v + m_terms * (8 * W + w_c) + j_groups * 8 * W
     peak, peak_kind = load_peaks()
     achieved = bytes_alg / (t_local / args.steps) / 1e9
-    traffic = load_traffic(args.workload, cache, layout, args.precision)
+    traffic, traffic_note = load_traffic(args.workload, cache, layout, args.precision)
+    dram_frac = None
+    if traffic is not None:
+        dram_frac = traffic / (t_local / args.steps) / 1e9 / peak
     props = torch.cuda.get_device_properties(dev)
     sm_mhz = clocks['sm_mhz'] if clocks and clocks.get('sm_mhz') else 1965.0
     issue = None
@@ -378,6 +418,8 @@ def run_ours(args):
                        'setup_s': setup_s},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                          'frac': achieved / peak, 'traffic': traffic,
+                         'traffic_source': traffic_note,
+                         'dram_frac': dram_frac,
                          'peak_kind': peak_kind,
                          'bytes_alg_per_launch': bytes_alg,
                          'formula': 'N(8W+2w_v) + P_valid w_v + M(8W+w_c) + J 8W, W=1, '

@@ -228,6 +228,14 @@ int sqd_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xini
              int mode, int use_graph, void* stream, double* eigval_host, void* eigvec,
              int* niter_host, double* residual_host);
 
+/* eigenpair_2x2 / eigenpair_3x3 (ground_locg.py:467-514): the lowest eigenpair of each of
+ * `count` Hermitian dim x dim matrices (dim 2: closed form; dim 3: Cardano's method after Kopp
+ * 2008, eigenvector from a cross product), with the device routines the solver's Rayleigh-Ritz
+ * steps use.  mats: complex128 row-major [count, dim, dim]; vals: [count] doubles; vecs:
+ * complex128 [count, dim].  Stream-ordered; no synchronization. */
+int sqd_eigenpair_small(const void* mats, int64_t count, int dim, double* vals, void* vecs,
+                        void* stream);
+
 /* ---------------------------------------------------------------- batched instances -------- */
 /* Many independent SQD problems solved together (no rqutils counterpart: rqutils solves one
  * subspace per call).  The operators' stored pairs (cache_strategy (1, 2) required) are copied

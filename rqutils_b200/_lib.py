@@ -58,6 +58,7 @@ PROTOTYPES = {
     'sqd_locg': (_i32, [_i64, _i32, _vp, _vp, _vp, _i64, _c.POINTER(_vp), _i32, _f64, _i32,
                         _i32, _i32, _vp, _c.POINTER(_f64), _vp, _c.POINTER(_i32),
                         _c.POINTER(_f64)]),
+    'sqd_eigenpair_small': (_i32, [_vp, _i64, _i32, _vp, _vp, _vp]),
 }
 # Library extensions beyond the header's core set (declared in the header as well).
 EXTRA_PROTOTYPES = {

@@ -2063,3 +2063,45 @@ extern "C" int sqd_batch_locg(sqd_batch_t b, int dtype, const void* xinit,
 }
 
 extern "C" void sqd_batch_destroy(sqd_batch_t b) { delete b; }
+
+// ----------------------------------------------------------------------------- small eigenpairs
+// eigenpair_2x2 / eigenpair_3x3 (ground_locg.py:467-514) on a batch of Hermitian matrices, one
+// thread per matrix: the same device functions the Rayleigh-Ritz steps of the solver call.
+namespace sqd {
+namespace {
+__global__ void k_eigenpair_small(const double2* __restrict__ mats, int64_t count, int dim,
+                                  double* __restrict__ vals, double2* __restrict__ vecs) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const double2* m = mats + i * dim * dim;
+  if (dim == 2) {
+    double2 a[2][2] = {{m[0], m[1]}, {m[2], m[3]}};
+    double2 v[2];
+    eig2(a, &vals[i], v);
+    vecs[i * 2] = v[0];
+    vecs[i * 2 + 1] = v[1];
+  } else {
+    double2 a[3][3] = {{m[0], m[1], m[2]}, {m[3], m[4], m[5]}, {m[6], m[7], m[8]}};
+    double2 v[3];
+    eig3(a, &vals[i], v);
+    for (int k = 0; k < 3; ++k) vecs[i * 3 + k] = v[k];
+  }
+}
+}  // namespace
+}  // namespace sqd
+
+extern "C" int sqd_eigenpair_small(const void* mats, int64_t count, int dim, double* vals,
+                                   void* vecs, void* stream) {
+  return guarded([&] {
+    SQD_REQUIRE(dim == 2 || dim == 3, "dim must be 2 or 3");
+    SQD_REQUIRE(count >= 0, "negative count");
+    if (count == 0) return;
+    SQD_REQUIRE(mats != nullptr && vals != nullptr && vecs != nullptr, "NULL array");
+    const int threads = 128;
+    const int64_t blocks = (count + threads - 1) / threads;
+    SQD_REQUIRE(blocks <= 0x7fffffff, "count too large");
+    k_eigenpair_small<<<(unsigned)blocks, threads, 0, as_stream(stream)>>>(
+        static_cast<const double2*>(mats), count, dim, vals, static_cast<double2*>(vecs));
+    SQD_CHECK_LAUNCH();
+  });
+}

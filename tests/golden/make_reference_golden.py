@@ -83,7 +83,8 @@ class Recorder:
     def __call__(self, matvec, xinit, args=(), orth=(), maxiter=1000, tol=None, vspace=None,
                  log_level=logging.WARNING):
         self.vinit = int(np.asarray(xinit))
-        self.hv = np.stack([np.asarray(matvec(p, *args)) for p in self.probes])
+        self.hv = (np.stack([np.asarray(matvec(p, *args)) for p in self.probes])
+                   if len(self.probes) else None)
         if not self.solve:
             raise _Stop()
         e, v, it = self.real(matvec, xinit, args=args, orth=orth, maxiter=maxiter, tol=tol,
@@ -157,11 +158,12 @@ def subspace_case(R, rec):
     out['xsource_unsorted'] = np.stack([np.asarray(R.sqd.get_xsource(xx, usp,
                                                                      sorted_input=False))
                                         for xx in ham.x])
-    probes = np.stack([rng.standard_normal(200) + 1j * rng.standard_normal(200)
+    # run_sqd on all 240 samples with states_size 260: 180 unique rows and 80 fill rows
+    probes = np.stack([rng.standard_normal(260) + 1j * rng.standard_normal(260)
                        for _ in range(2)])
     out['probes'] = probes
     for cache in ((1, 0), (1, 2), (0, 0), (0, 2)):
-        run_sqd_capture(R, rec, (labels, list(c)), bits, 200, cache, probes)
+        run_sqd_capture(R, rec, (labels, list(c)), bits, 260, cache, probes)
         out[f'hv_{cache[0]}{cache[1]}'] = rec.hv
         out[f'vinit_{cache[0]}{cache[1]}'] = np.array(rec.vinit)
     return out
@@ -206,7 +208,7 @@ def real_solves(R, rec):
     rng = np.random.default_rng(505)
     samples = np.concatenate([wl.states, rng.choice(wl.states, size=50)])
     rng.shuffle(samples)
-    cases.append(('jw6', wl.x, wl.z, wl.coeffs, 12, samples, 420))
+    cases.append(('jw6', wl.x, wl.z, wl.coeffs, 12, samples, 470))
     # random even-Y Pauli sum on 12 qubits, 500 weight-6 strings
     x, z, c = even_y_pauli_sum(12, 200, rng)
     cases.append(('evy12', x, z, c, 12, W.weight_subspace(12, 6, 500, rng), None))
@@ -233,7 +235,7 @@ def real_solves(R, rec):
     tag, x, z, c, n, samples, size = cases[0]
     labels = W.labels_from_xz(x, z, n)
     e, vec, _ = run_sqd_capture(R, rec, (labels, list(c)), bits_of(samples, n), size, (1, 0),
-                                probes[:, :0], solve=True, maxiter=12)
+                                probes[:0], solve=True, maxiter=12)
     out['jw6_cap12_energy'] = np.array(e)
     out['jw6_cap12_niter'] = np.array(rec.niter)
     out['jw6_cap12_eigvec'] = np.asarray(vec)

@@ -3,15 +3,44 @@ formula, workload naming."""
 import bench
 
 
-def test_traffic_follows_the_chosen_layout():
-    csr = bench.load_traffic('c2', (1, 2), 'csr')
-    prod_csr = bench.load_traffic('c2', (1, 2), 'product-csr')
-    prod = bench.load_traffic('c2', (1, 2), 'product')
-    assert csr is not None and prod_csr is not None
-    assert prod_csr < csr                 # the slabs read fewer bytes than the pair lists
-    assert prod == prod_csr               # falls back to the other product summary
-    assert bench.load_traffic('c3', (1, 2), 'product') > 1e10
-    assert bench.load_traffic('c1', (1, 2), 'csr') is None
+def _profiles(tmp_path, files):
+    (tmp_path / 'profiles').mkdir()
+    for name, text in files.items():
+        (tmp_path / 'profiles' / name).write_text(text)
+
+
+def test_traffic_follows_the_chosen_layout_and_current_sources(tmp_path, monkeypatch):
+    monkeypatch.setattr(bench, 'ROOT', str(tmp_path))
+    monkeypatch.setattr(bench, 'kernel_sources_digest', lambda: 'abc')
+    _profiles(tmp_path, {
+        'matvec_c2_cache12.md': 'traffic_bytes_per_launch: 300\nkernel_sources_sha256: abc\n',
+        'matvec_c2_cache12_product-csr.md':
+            'x\ntraffic_bytes_per_launch: 200\nkernel_sources_sha256: abc\n',
+        'matvec_c3_cache12_product.md': 'traffic_bytes_per_launch: 9\nkernel_sources_sha256: old\n',
+    })
+    assert bench.load_traffic('c2', (1, 2), 'csr')[0] == 300
+    assert bench.load_traffic('c2', (1, 2), 'product-csr')[0] == 200
+    # the product layout falls back to the other product summary
+    assert bench.load_traffic('c2', (1, 2), 'product')[0] == 200
+    # a capture of other kernel sources is not used
+    val, note = bench.load_traffic('c3', (1, 2), 'product')
+    assert val is None and 'other kernel sources' in note
+    assert bench.load_traffic('c1', (1, 2), 'csr')[0] is None
+    # FP32 vectors use their own summaries
+    assert bench.load_traffic('c2', (1, 2), 'product-csr', 'fp32')[0] is None
+
+
+def test_kernel_sources_digest_is_stable():
+    assert bench.kernel_sources_digest() == bench.kernel_sources_digest()
+    assert len(bench.kernel_sources_digest()) == 64
+
+
+def test_cpu_sample_is_shared_and_seeded():
+    wl = bench.make_workload('c1')
+    a = bench.cpu_sample(wl)
+    b = bench.cpu_sample(wl)
+    assert (a == b).all() and a.shape[0] == 2000 and (a[1:] > a[:-1]).all()
+    assert bench.cpu_sample(wl, rows=100).shape[0] == 100
 
 
 def test_locg_bytes_formula():
@@ -44,8 +73,3 @@ def test_issue_bound_estimate():
     assert b['cached_fp64_fma_floor_ms'] < 0.1 * b['timed_matvec_ms']
     assert bench.issue_bound(n, m, p, True, 148, 1965.0, 6.0e-3)['cached_fp64_fma_per_matvec'] \
         == 4 * p
-
-
-def test_fp32_traffic_uses_its_own_summaries():
-    assert bench.load_traffic('c2', (1, 2), 'product-csr', 'fp32') is None
-    assert bench.load_traffic('c2', (1, 2), 'product-csr', 'fp64') is not None
