@@ -66,6 +66,11 @@ const char* sqd_last_error(void);
  * owns device memory).  This releases all but keep_bytes of the current device's pool back to
  * the driver (synchronizes the device). */
 int sqd_trim_memory(uint64_t keep_bytes);
+/* Usage of that pool on the current device (no counterpart in rqutils): bytes reserved from the
+ * driver, bytes in live allocations, and the high-water mark of the latter, which reset_high
+ * != 0 first resets to the current usage.  Any output pointer may be NULL. */
+int sqd_memory_stats(uint64_t* reserved_host, uint64_t* used_host, uint64_t* used_high_host,
+                     int reset_high);
 
 /* ---------------------------------------------------------------- Pauli sums --------------- */
 /* PauliSumXZ.from_paulisum (paulis/symplectic.py:50-124), on the device: drops zero
@@ -177,8 +182,11 @@ int sqd_vinit(sqd_op_t op, int64_t* index_host, void* stream);
  * live in a fixed file-scope __device__ array (256 KiB, held by every GPU that loads the
  * library until exit) instead of a per-call cudaMallocAsync.  Limit: 67,108,864 real rows,
  * larger subspaces return SQD_ERR_INVALID.  The array is shared by all calls, so calls whose
- * GPU work overlaps race; the first call on a device resolves the array's address and should
- * come before any stream capture. */
+ * GPU work overlaps race.  Set-up: the first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress, once per device) and keeps it; make that first call before
+ * any stream capture begins, and do not use the function on a device after cudaDeviceReset
+ * (the kept address then belongs to the destroyed context).  Every call synchronizes `stream`
+ * and writes the index to the host. */
 int sqd_vinit_noalloc(sqd_op_t op, int64_t* index_host, void* stream);
 /* Projected matrix <i|H|j> in CSR (hproj, sqd.py:269-314, with its padding bug fixed):
  * indptr[states_size+1] (int64), indices[nnz] (int32), data[nnz] complex128 (interleaved). */
@@ -235,6 +243,15 @@ int sqd_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xini
  * complex128 [count, dim].  Stream-ordered; no synchronization. */
 int sqd_eigenpair_small(const void* mats, int64_t count, int dim, double* vals, void* vecs,
                         void* stream);
+
+/* Per-iteration record of the NEXT sqd_locg call on the calling thread: the values behind the
+ * reference's log_level <= DEBUG prints (ground_locg.py:330-331, 377-378).  After that call
+ * returns, rows_host holds *count_host rows (at most max_rows) of 6 doubles: phase (0 = FP64
+ * iteration, 1 = FP32 sweep of the mixed solver, which come first), iteration number, theta,
+ * |r|, reltol = (|Ax| - theta) * 10 n (FP32 sweeps: their stopping threshold
+ * 2e-7 |theta|), converged (0/1).  Recording costs one store per iteration.  rows_host = NULL
+ * or max_rows = 0 cancels a pending request. */
+int sqd_locg_record(double* rows_host, int64_t max_rows, int64_t* count_host);
 
 /* ---------------------------------------------------------------- batched instances -------- */
 /* Many independent SQD problems solved together (no rqutils counterpart: rqutils solves one

@@ -9,18 +9,17 @@ Each function cites the reference file:line it restates (paths relative to the r
 
 Parity status
 -------------
-The reference is pure Python on JAX and JAX is not installed in this image, so the reference's
-own functions cannot be executed here, and the reference ships no golden vectors (its only test,
-``tests/sqd.ipynb``, compares ``sqd`` against a dense ``eigh`` of the projected Qiskit matrix and
-has no stored outputs).  The restatement is therefore pinned in two independent ways:
+Pinned to the reference's own execution.  The reference is pure Python on JAX, which is not
+installed in this image; ``tests/golden/make_reference_golden.py`` imports the UNMODIFIED
+reference modules through a NumPy stand-in for the JAX subset they use
+(``tests/golden/jax_stand_in``) and records their outputs as ``tests/golden/reference_*.npz``.
+``tests/test_reference_golden.py`` and ``tests/test_oracle_cpu_baseline.py`` check this
+restatement against them: Pauli tables, uniquified rows and indices, source indices, group
+diagonals and start indices bit for bit; matvecs, energies and small eigenpairs to written
+tolerances.  Also kept: the independent dense Kronecker-product construction
+(``oracle.dense``) with ``numpy.linalg.eigh``, the check of the reference's notebook.
 
-* against a dense Kronecker-product construction of every Pauli string (``oracle.dense``), which
-  is independent of the symplectic bit tricks, and ``numpy.linalg.eigh`` of the projected matrix
-  — the same check the reference's notebook performs;
-* against the literal sort-based ``get_xsource`` algorithm (restated step by step), for bit-exact
-  connectivity.
-
-What is NOT pinned: the exact floating-point summation order of XLA's reductions inside
-``ground_locg`` (``jnp.sum``/``jnp.linalg.norm``).  That boundary is "parity unpinned"; results
-are compared with tolerances there.
+What is NOT pinned: XLA's floating-point summation order inside ``jnp.sum`` /
+``jnp.linalg.norm`` (the stand-in sums in NumPy's order); results are compared with tolerances
+there.
 """

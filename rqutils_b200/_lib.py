@@ -59,6 +59,7 @@ PROTOTYPES = {
                         _i32, _i32, _vp, _c.POINTER(_f64), _vp, _c.POINTER(_i32),
                         _c.POINTER(_f64)]),
     'sqd_eigenpair_small': (_i32, [_vp, _i64, _i32, _vp, _vp, _vp]),
+    'sqd_locg_record': (_i32, [_vp, _i64, _c.POINTER(_i64)]),
 }
 # Library extensions beyond the header's core set (declared in the header as well).
 EXTRA_PROTOTYPES = {
@@ -66,6 +67,7 @@ EXTRA_PROTOTYPES = {
     'sqd_op_get_lanes': (_i32, [_vp, _i32, _c.POINTER(_i32)]),
     'sqd_vinit_noalloc': (_i32, [_vp, _c.POINTER(_i64), _vp]),
     'sqd_trim_memory': (_i32, [_u64]),
+    'sqd_memory_stats': (_i32, [_c.POINTER(_u64), _c.POINTER(_u64), _c.POINTER(_u64), _i32]),
     'sqd_paulis_set_coeffs': (_i32, [_vp, _vp, _vp, _vp, _c.POINTER(_i32)]),
     'sqd_op_refresh': (_i32, [_vp, _vp]),
     'sqd_batch_create': (_i32, [_c.POINTER(_vp), _i32, _vp, _c.POINTER(_vp)]),
@@ -122,6 +124,13 @@ def call(name, *args):
 def trim_memory(keep_bytes=0):
     """Return the library's cached device memory to the driver."""
     call('sqd_trim_memory', int(keep_bytes))
+
+
+def memory_stats(reset_high=False):
+    """(reserved, used, used_high) bytes of the library's memory pool on the current device."""
+    vals = [_u64(0), _u64(0), _u64(0)]
+    call('sqd_memory_stats', *(_c.byref(v) for v in vals), int(bool(reset_high)))
+    return tuple(int(v.value) for v in vals)
 
 
 def require_cuda():

@@ -43,6 +43,30 @@ extern "C" int sqd_trim_memory(uint64_t keep_bytes) {
   });
 }
 
+extern "C" int sqd_memory_stats(uint64_t* reserved_host, uint64_t* used_host,
+                                uint64_t* used_high_host, int reset_high) {
+  return sqd::guarded([&] {
+    cudaMemPool_t pool = sqd::library_pool();
+    uint64_t v = 0;
+    if (reset_high) {
+      uint64_t zero = 0;      // resets the high-water mark to the current usage
+      SQD_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &zero));
+    }
+    if (reserved_host) {
+      SQD_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &v));
+      *reserved_host = v;
+    }
+    if (used_host) {
+      SQD_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &v));
+      *used_host = v;
+    }
+    if (used_high_host) {
+      SQD_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &v));
+      *used_high_host = v;
+    }
+  });
+}
+
 extern "C" const char* sqd_version(void) { return "sqd_b200 0.1.0 (sm_100a)"; }
 
 extern "C" const char* sqd_last_error(void) { return sqd::g_last_error.c_str(); }

@@ -75,7 +75,18 @@ struct LocgDev {
   int keep;              // project_out mask result
   int rzero;
   int stall;             // stop after this many iterations without improving |r| (0 = never)
+  // Per-iteration record (the reference's log_level <= DEBUG prints, ground_locg.py:330-331,
+  // 377-378): rows of kHistCols doubles written by the convergence step while hist_n <
+  // hist_cap; hist == nullptr records nothing.
+  double* hist;
+  int hist_cap;
+  int hist_n;
+  int hist_phase;        // first column of every row: 0 = FP64 iteration, 1 = FP32 sweep
 };
+
+// Columns of a history row: phase, iteration, theta, |r|, reltol ((|Ax| - theta) * 10 N; the
+// FP32 sweeps store their stopping threshold inner_rtol * |theta| there), converged.
+constexpr int kHistCols = 6;
 
 enum Gate : int { G_NONE = 0, G_DONE = 1, G_KEEP = 2 };
 
@@ -178,19 +189,31 @@ __device__ void conv_step(LocgDev* d, double ax2, int use_cond, cudaGraphConditi
   d->rnorm = r;
   d->niter += 1;
   bool conv;
+  double reltol;
   if (d->inner_rtol > 0.0) {
-    conv = r < d->inner_rtol * fabs(d->theta);
+    reltol = d->inner_rtol * fabs(d->theta);
+    conv = r < reltol;
     if (r < 0.5 * d->best_r) {
       d->best_r = r;
       d->best_it = d->niter;
     }
     if (d->stall > 0 && d->niter - d->best_it > d->stall) conv = true;
   } else {
-    const double reltol = (sqrt(ax2) - d->theta) * d->nscale;
+    reltol = (sqrt(ax2) - d->theta) * d->nscale;
     conv = r < d->tol * reltol;
   }
   if (d->etol > 0.0 && d->niter >= 2 && fabs(d->theta - d->theta_prev) <= d->etol * fabs(d->theta))
     conv = true;
+  if (d->hist != nullptr && d->hist_n < d->hist_cap) {
+    double* row = d->hist + static_cast<int64_t>(d->hist_n) * kHistCols;
+    row[0] = d->hist_phase;
+    row[1] = d->niter;
+    row[2] = d->theta;
+    row[3] = r;
+    row[4] = reltol;
+    row[5] = conv ? 1.0 : 0.0;
+    d->hist_n += 1;
+  }
   d->converged = conv;
   d->done = conv || d->niter >= d->maxiter;
   if (use_cond) cudaGraphSetConditional(cond, d->done ? 0u : 1u);
@@ -765,9 +788,20 @@ class Locg {
   // every solve ends with a stream synchronisation).
   void set_stream(cudaStream_t st) { st_ = cur_ = st; }
 
+  // Where the next solve records its iterations (nullptr: nothing); takes effect at
+  // set_params.
+  void set_history(double* rows, int cap, int phase) {
+    hist_ = rows;
+    hist_cap_ = cap;
+    hist_phase_ = phase;
+  }
+
   void set_params(double tol, double nscale, int maxiter, double inner_rtol, double etol,
                   int stall) {
     LocgDev h{};
+    h.hist = hist_;
+    h.hist_cap = hist_cap_;
+    h.hist_phase = hist_phase_;
     h.tol = tol;
     h.nscale = nscale;
     h.maxiter = maxiter;
@@ -1116,6 +1150,9 @@ class Locg {
   void* ctx_;
   cudaStream_t st_;
   cudaStream_t cur_;  // launch stream: st_, or the private capture stream while capturing
+  double* hist_ = nullptr;
+  int hist_cap_ = 0;
+  int hist_phase_ = 0;
   unsigned blocks_ = 1;
   DevBuf<double> partials_;
   DevBuf<unsigned> counter_;
@@ -1177,6 +1214,42 @@ SolverCache<NC>* solver_cache(sqd_op_s* op, int64_t n) {
   return c;
 }
 
+// Iteration record requested by sqd_locg_record for the next sqd_locg call on this thread.
+struct HistRequest {
+  double* rows_host = nullptr;
+  int64_t max_rows = 0;
+  int64_t* count_host = nullptr;
+};
+thread_local HistRequest g_hist_request;
+
+// Device rows for one solver object; copied to the caller's host rows after the solve.
+struct HistRecorder {
+  HistRequest req;
+  DevBuf<double> rows[2];   // [0] FP64, [1] FP32
+  void arm(int phase, cudaStream_t st) {
+    rows[phase].alloc(static_cast<size_t>(req.max_rows) * kHistCols, st);
+  }
+  // Copies FP32 rows (they come first in time) then FP64 rows, up to max_rows in total.
+  template <class L64, class L32>
+  void finish(L64* l64, L32* l32, cudaStream_t st) {
+    int64_t written = 0;
+    auto take = [&](auto* l, int phase) {
+      if (!l || !rows[phase].ptr) return;
+      l->read_host();
+      const int64_t n = std::min<int64_t>(l->host().hist_n, req.max_rows - written);
+      if (n > 0)
+        SQD_CUDA(cudaMemcpyAsync(req.rows_host + written * kHistCols, rows[phase].ptr,
+                                 sizeof(double) * kHistCols * n, cudaMemcpyDeviceToHost, st));
+      written += std::max<int64_t>(n, 0);
+      l->set_history(nullptr, 0, 0);
+    };
+    take(l32, 1);
+    take(l64, 0);
+    SQD_CUDA(cudaStreamSynchronize(st));
+    if (req.count_host) *req.count_host = written;
+  }
+};
+
 // cache_op: the sqd operator behind fn (NULL for a caller's own matvec), whose solver cache
 // the FP64 path may use.
 template <int NC>
@@ -1200,6 +1273,11 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, sqd_op_s* cache
       lp = own.get();
     }
     Locg<double, NC>& L = *lp;
+    HistRecorder rec{g_hist_request};
+    g_hist_request = HistRequest{};
+    if (rec.req.rows_host) rec.arm(0, st);
+    // always set: a cached solver must not keep a previous solve's (freed) record buffer
+    L.set_history(rec.rows[0].ptr, static_cast<int>(rec.req.max_rows), 0);
     L.set_params(tol < 0 ? eps64 : tol, nscale, maxiter, 0.0, 0.0, 0);
     if (xinit)
       SQD_CUDA(cudaMemcpyAsync(L.x(), xinit, sizeof(double) * NC * n, cudaMemcpyDeviceToDevice,
@@ -1217,6 +1295,7 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, sqd_op_s* cache
     SQD_CUDA(cudaMemcpyAsync(eigvec, L.x(), sizeof(double) * NC * n, cudaMemcpyDeviceToDevice,
                              st));
     SQD_CUDA(cudaStreamSynchronize(st));
+    if (rec.req.rows_host) rec.finish(&L, static_cast<Locg<float, NC>*>(nullptr), st);
     return;
   }
   // Mixed precision.
@@ -1275,6 +1354,15 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, sqd_op_s* cache
   int it32 = 0;
   Locg<double, NC>& L = *l64;
   L.set_stream(st);
+  HistRecorder rec{g_hist_request};
+  g_hist_request = HistRequest{};
+  if (rec.req.rows_host) {
+    rec.arm(0, st);
+    rec.arm(1, st);
+  }
+  // always set: a cached solver must not keep a previous solve's (freed) record buffer
+  L.set_history(rec.rows[0].ptr, static_cast<int>(rec.req.max_rows), 0);
+  l32->set_history(rec.rows[1].ptr, static_cast<int>(rec.req.max_rows), 1);
   {
     Locg<float, NC>& L32 = *l32;
     L32.set_stream(st);
@@ -1336,6 +1424,7 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, sqd_op_s* cache
   SQD_CUDA(cudaMemcpyAsync(eigvec, L.x(), sizeof(double) * NC * n, cudaMemcpyDeviceToDevice,
                            st));
   SQD_CUDA(cudaStreamSynchronize(st));
+  if (rec.req.rows_host) rec.finish(&L, l32, st);
 }
 
 }  // namespace
@@ -1893,6 +1982,16 @@ int op_dtype_cb(void* ctx, const void* x, void* y, void* stream) {
   return guarded([&] { op_matvec(c->op, x, y, c->dtype, as_stream(stream)); });
 }
 }  // namespace
+
+extern "C" int sqd_locg_record(double* rows_host, int64_t max_rows, int64_t* count_host) {
+  return guarded([&] {
+    SQD_REQUIRE(max_rows >= 0 && max_rows <= (1 << 24), "max_rows must be in [0, 2^24]");
+    g_hist_request = HistRequest{};
+    if (rows_host == nullptr || max_rows == 0) return;
+    g_hist_request = HistRequest{rows_host, max_rows, count_host};
+    if (count_host) *count_host = 0;
+  });
+}
 
 extern "C" int sqd_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, const void* xinit,
                         int64_t xinit_index, const void* const* orth, int n_orth, double tol,

@@ -153,7 +153,10 @@ __global__ void k_diagonal(const uint64_t* states, int64_t n_unique, uint64_t fi
   }
 }
 
+// Order-preserving map of a double onto unsigned integers; -0.0 maps like +0.0 (the two compare
+// equal, and jnp.argmin at sqd.py:413 keeps the first of equal values).
 __device__ __forceinline__ unsigned long long order_key(double v) {
+  if (v == 0.0) v = 0.0;
   unsigned long long b = __double_as_longlong(v);
   return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
 }

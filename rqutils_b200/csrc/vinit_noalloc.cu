@@ -17,11 +17,12 @@
 //    subspaces are rejected with SQD_ERR_INVALID and a message naming the limit.
 //  * All calls on a device share the array: calls whose GPU work overlaps (different streams,
 //    or several host threads) race and must be serialised by the caller.
-//  * The first call on each device resolves the array's device address with
-//    cudaGetSymbolAddress (with that device current) and caches it; that first call should
-//    come before any stream capture.
-//  * No cudaMalloc / cudaFree / allocating library call; the result is returned to the host
-//    (the call synchronises `stream`).
+//  * Set-up: the first call on each device resolves the array's device address with
+//    cudaGetSymbolAddress (with that device current) and keeps it for the process; make that
+//    first call before any stream capture begins.  After cudaDeviceReset the kept address
+//    belongs to the destroyed context, so the function must not be used on that device again.
+//  * No cudaMalloc / cudaFree / allocating library call; every call synchronises `stream` and
+//    returns the index to the host.
 #include <mutex>
 
 #include "internal.cuh"
@@ -58,8 +59,10 @@ __device__ __forceinline__ double na_diag0(const int64_t* gs, const int32_t* ge,
   return d;
 }
 
-// Order-preserving map of a double onto unsigned integers.
+// Order-preserving map of a double onto unsigned integers; -0.0 maps like +0.0, so the two
+// tie and the smaller row index wins, as in jnp.argmin (sqd.py:413).
 __device__ __forceinline__ unsigned long long na_key(double v) {
+  if (v == 0.0) v = 0.0;
   const unsigned long long b = __double_as_longlong(v);
   return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
 }

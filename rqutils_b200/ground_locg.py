@@ -12,6 +12,13 @@ has the reference's signature and meaning (ground_locg.py:128-162) and returns
 
 Two B200 extensions: ``mode='mixed'`` (FP32 sweeps + FP64 refinement, SQD operators only) and
 ``use_graph``.
+
+``log_level <= logging.DEBUG`` prints the reference's per-iteration lines (ground_locg.py:330-331,
+377-378: ``LOCG iteration {i}`` and ``Residual {r}, reltol {reltol}, converged: {c}``) after the
+solve, from a record the device solver writes as it iterates (the loop itself runs on the GPU;
+FP32 sweeps of the mixed solver print as ``FP32 sweep {i}`` lines first).  The rows are kept in
+``ground_locg.last_history``: an array of (phase, iteration, theta, |r|, reltol, converged), phase
+0 for FP64 iterations and 1 for FP32 sweeps.
 """
 import logging
 
@@ -103,6 +110,14 @@ def ground_locg(mat, xinit, args=(), orth=(), maxiter=1000, tol=None, vspace=Non
     nit = _lib._i32()
     res = _lib._f64()
     vec = torch.empty(n, dtype=dtype, device=dev)
+    record = log_level <= logging.DEBUG
+    if record:
+        max_rows = 2 * int(maxiter) + 64
+        rows = np.zeros((max_rows, 6), dtype=np.float64)
+        count = _lib._i64(0)
+        _lib.call('sqd_locg_record', rows.ctypes.data_as(_lib._vp), max_rows,
+                  _lib._c.byref(count))
+        print('Performing first LOBPCG steps', flush=True)
     status = _lib.load().sqd_locg(
         n, code, fn, ctx, _lib.ptr(xinit_t), xinit_index, orth_arr, len(orth_t),
         -1.0 if tol is None else float(tol), int(maxiter), mode_code, 1 if use_graph else 0,
@@ -110,9 +125,26 @@ def ground_locg(mat, xinit, args=(), orth=(), maxiter=1000, tol=None, vspace=Non
         _lib._c.byref(res))
     if not isinstance(mat, SQDOperator) and errors:
         raise errors[0]
+    if status != _lib.SQD_OK and record:
+        _lib.call('sqd_locg_record', _lib._vp(0), 0, None)
     _lib.check(status)
     ground_locg.last_residual = res.value
+    if record:
+        ground_locg.last_history = rows[:count.value].copy()
+        _print_history(ground_locg.last_history)
     return eig.value, vec, nit.value
+
+
+def _print_history(rows):
+    """The reference's debug lines (ground_locg.py:330-331, 377-378), one iteration each."""
+    for phase, it, theta, r, reltol, conv in rows:
+        if phase == 1:
+            print(f'FP32 sweep {int(it) - 1}', flush=True)
+            print(f'Residual {r}, target {reltol}, theta {theta}, converged: {bool(conv)}',
+                  flush=True)
+        else:
+            print(f'LOCG iteration {int(it) - 1}', flush=True)
+            print(f'Residual {r}, reltol {reltol}, converged: {bool(conv)}', flush=True)
 
 
 def _torch_dtype(dt):

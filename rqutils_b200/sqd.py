@@ -38,7 +38,22 @@ _LOOKUPS = {'hash': _lib.SQD_LOOKUP_HASH, 'bsearch': _lib.SQD_LOOKUP_BSEARCH,
 
 @dataclass(frozen=True)
 class SQDOptions:
-    """Options of ``sqd`` (sqd.py:183-196) plus B200 extensions (after ``locg_tol``)."""
+    """Options of ``sqd`` (sqd.py:183-196) plus B200 extensions (after ``locg_tol``).
+
+    ``cache_strategy`` keeps the reference's meaning for what is cached, with two merges:
+
+    * ``(0, 1)`` and ``(0, 2)`` run as ``(0, 0)``: without cached sources every matvec looks the
+      sources up again, and the diagonal of each found pair is recomputed beside that lookup
+      from popcounts, so nothing is stored per pair (the reference stores sign bits or diagonals
+      for all N rows of every group, sqd.py:106-122).
+    * ``(1, 1)`` runs as ``(1, 0)``: the diagonals are recomputed from popcounts per stored pair
+      instead of from packed sign bits.  The reference's ``compute_diagonal`` reads the bit of
+      term t at ``t & 255`` instead of ``t & 7`` (sqd.py:590), so its (x, 1) results are wrong
+      for groups of more than 8 terms; these strategies give the correct diagonal.
+
+    All strategies give the same Hv (to rounding); they differ in memory and speed: ``(1, 2)``
+    stores one element per (row, group) pair whose source exists and is the fastest matvec.
+    """
     return_eigvec: bool = True
     cache_strategy: tuple[int, int] = (1, 0)
     shard_bundle: int = 1
@@ -331,21 +346,38 @@ def sqd(hamiltonian, states, states_size=None, options=None):
     return eigval
 
 
-def run_sqd(hamiltonian, states, states_size, options=None):
+def run_sqd(hamiltonian, states, states_size, options=None, log_level=logging.INFO):
     """run_sqd (sqd.py:317-442).  ``states``: binary [N, n] array, or a ``Subspace``.
-    Returns (eigval,) or (eigval, eigvec, space, subspace_dim)."""
+    Returns (eigval,) or (eigval, eigvec, space, subspace_dim).
+
+    ``log_level <= logging.DEBUG`` prints the reference's progress lines (sqd.py:338-430) and
+    the solver's per-iteration lines.  (The reference's own ``jax.debug.print(ordered=True)(...)``
+    calls there pass no format string to ``jax.debug.print`` and raise at that level.)"""
     if options is None:
         options = SQDOptions()
+    debug = log_level <= logging.DEBUG
     hamiltonian = _as_pauli(hamiltonian)
+    if debug:
+        print(f'Uniquifying states (size {states_size})', flush=True)
     space = states if isinstance(states, Subspace) else Subspace.from_bits(states, states_size)
+    if debug and options.cache_strategy[0] > 0:
+        print('Precomputing xsources', flush=True)
+    if debug and options.cache_strategy == (1, 2):
+        print('Precomputing diagonals', flush=True)
     op = SQDOperator(hamiltonian, space, options.cache_strategy, options.lookup,
                      options.lanes_per_row)
     if options.autotune and options.lanes_per_row is None:
         op.autotune()
+    if debug:
+        print('Generating vinit', flush=True)
     vinit = op.vinit()
+    if debug:
+        print(f'Starting minimization with cache_strategy {tuple(options.cache_strategy)}',
+              flush=True)
     eigval, eigvec, _ = ground_locg(op, vinit, maxiter=options.locg_maxiter,
                                     tol=options.locg_tol, vspace=(space.states_size, op.dtype),
-                                    mode=options.locg_mode, use_graph=options.use_graph)
+                                    log_level=log_level, mode=options.locg_mode,
+                                    use_graph=options.use_graph)
     result = (eigval,)
     if options.return_eigvec:
         result += (eigvec, space, space.n_unique)

@@ -199,3 +199,43 @@ def test_small_eigenpairs_match_reference_and_eigh():
 def test_small_eigenpairs_reject_bad_dimensions():
     st = _lib.load().sqd_eigenpair_small(None, 1, 4, None, None, None)
     assert st == _lib.SQD_ERR_INVALID
+
+
+def test_debug_log_level_records_and_prints_every_iteration(capsys):
+    """log_level=DEBUG: the reference's per-iteration lines (ground_locg.py:330-331, 377-378),
+    from the record the device solver writes; the residual sequence follows the oracle's
+    iteration of the same algorithm (FP64, another summation order) step by step."""
+    import logging
+    from oracle import symplectic as OS, sqd as OQ, ground_locg as OL
+    g = load('reference_solves')
+    lab, c, bits = labels(g['jw6_labels']), list(g['jw6_coeffs']), g['jw6_bits']
+    size = int(g['jw6_size'])
+    ham = rq.PauliSumXZ.from_paulisum((lab, c), force_real=True, add_padding=True)
+    op = rq.SQDOperator(ham, rq.Subspace.from_bits(bits, size))
+    capsys.readouterr()
+    e, _, niter = rq.ground_locg(op, op.vinit(), vspace=(op.size, torch.float64),
+                                 log_level=logging.DEBUG)
+    out = capsys.readouterr().out
+    hist = rq.ground_locg.last_history
+    assert out.count('LOCG iteration') == niter == hist.shape[0]
+    assert (hist[:, 0] == 0).all() and (hist[:, 1] == np.arange(1, niter + 1)).all()
+    assert hist[-1, 5] == 1 and (hist[:-1, 5] == 0).all() and hist[-1, 2] == e
+    oham = OS.from_paulisum((lab, c), force_real=True, add_padding=True)
+    su = OQ.uniquify_states(OQ.pack_states(bits), size)
+    xs = np.stack([OQ.get_xsource(x, su) for x in oham.x])
+    *_, hist_o = OL.ground_locg(lambda v: OQ.apply_h_x_cached(v, xs, oham.z, oham.c, su),
+                                OQ.vinit_index(oham, su), vspace=(size, np.float64),
+                                return_history=True)
+    k = min(30, niter)
+    np.testing.assert_allclose(hist[:k, 3], hist_o[:k], rtol=1e-6)
+    # mixed precision: FP32 sweeps first (phase 1), then FP64 iterations (phase 0)
+    e_m, _, niter_m = rq.ground_locg(op, op.vinit(), vspace=(op.size, torch.float64),
+                                     mode='mixed', log_level=logging.DEBUG)
+    hist_m = rq.ground_locg.last_history
+    phases = hist_m[:, 0]
+    assert hist_m.shape[0] == niter_m and phases[0] == 1
+    assert (np.diff(phases) <= 0).all()          # 1 ... 1 0 ... 0
+    assert hist_m[-1, 5] == 1 and abs(hist_m[-1, 2] - e_m) == 0
+    # no record without the debug level
+    rq.ground_locg(op, op.vinit(), vspace=(op.size, torch.float64))
+    assert 'LOCG iteration' not in capsys.readouterr().out

@@ -1,4 +1,5 @@
-"""sqd_vinit_noalloc, the allocation-free start-index search, checked against sqd_vinit.
+"""sqd_vinit_noalloc, the allocation-free start-index search, checked against sqd_vinit, the
+oracle's start index, and the library's memory pool.
 
 Callers whose device memory is fully reserved by their own allocator cannot let the library
 allocate; this entry point keeps its partial minima in a fixed __device__ array instead.  The
@@ -12,6 +13,7 @@ import torch
 
 import rqutils_b200 as rq
 from rqutils_b200 import _lib, workloads as W
+from oracle import symplectic as OS, sqd as OQ
 
 pytestmark = pytest.mark.gpu
 
@@ -67,3 +69,44 @@ def test_noalloc_vinit_null_operator_is_an_error():
     idx = ctypes.c_int64()
     st = _lib.load().sqd_vinit_noalloc(None, ctypes.byref(idx), None)
     assert st == _lib.SQD_ERR_INVALID
+
+
+def test_noalloc_vinit_matches_the_oracle_start_index():
+    """vinit of run_sqd (sqd.py:406-426) as the oracle restates it."""
+    for wl in (W.c1(0), W.c2_small(0, 96, 80)):
+        op = _operator(wl)
+        ham = OS.from_paulisum((wl.labels, list(wl.coeffs)), force_real=True, add_padding=True)
+        su = OQ.pack_states(OQ.u64_to_states(wl.states, wl.num_qubits))
+        assert _vinit('sqd_vinit_noalloc', op) == OQ.vinit_index(ham, su)
+
+
+def test_noalloc_vinit_ties_keep_the_first_row():
+    """Group 0 is a single Z on qubit 0: every odd state attains the minimum, and the first of
+    them (in sorted order) is the start index, as jnp.argmin returns the first minimum."""
+    states = np.array([2, 6, 7, 9, 12, 13, 15], dtype=np.uint64)
+    ham = rq.PauliSumXZ.from_xz(np.array([0, 3], dtype=np.uint64),
+                                np.array([1, 0], dtype=np.uint64), np.array([1.0, 0.25]), 4,
+                                force_real=True)
+    op = rq.SQDOperator(ham, rq.Subspace.from_u64(states, 4))
+    assert _vinit('sqd_vinit_noalloc', op) == _vinit('sqd_vinit', op) == 2
+
+
+def test_noalloc_vinit_allocates_nothing():
+    """Warm calls leave the library pool's reserved bytes, live bytes and high-water mark, and
+    torch's caching allocator, exactly as they were; the allocating sqd_vinit does move the
+    high-water mark, so the check can see an allocation."""
+    op = _operator(W.c2_small(0, 96, 80))
+    _vinit('sqd_vinit_noalloc', op)               # the first call on the device: set-up
+    torch.cuda.synchronize()
+    torch_before = (torch.cuda.memory_allocated(), torch.cuda.memory_reserved())
+    reserved0, used0, high0 = _lib.memory_stats(reset_high=True)
+    assert high0 == used0
+    for _ in range(3):
+        _vinit('sqd_vinit_noalloc', op)
+    torch.cuda.synchronize()
+    assert _lib.memory_stats() == (reserved0, used0, used0)
+    assert (torch.cuda.memory_allocated(), torch.cuda.memory_reserved()) == torch_before
+    _lib.memory_stats(reset_high=True)
+    _vinit('sqd_vinit', op)
+    torch.cuda.synchronize()
+    assert _lib.memory_stats()[2] > used0
