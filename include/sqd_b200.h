@@ -198,6 +198,12 @@ int sqd_grad_terms(sqd_op_t op, const void* u, const void* v, int dtype, double*
 /* Recomputes the cached matrix elements (cache z = 2) after sqd_paulis_set_coeffs; the
  * connectivity is unchanged. */
 int sqd_op_refresh(sqd_op_t op, void* stream);
+/* Turns an operator with cached sources and on-the-fly diagonals (cache_strategy (1, 0) or
+ * (1, 1)) into one with cached elements ((1, 2)): computes the element of every stored pair
+ * (8 bytes, 16 if complex), same values the on-the-fly matvec composes.  No rqutils counterpart
+ * (there the strategy is fixed when run_sqd builds its matvec); rqutils_b200.sqd uses it when
+ * the elements fit in device memory. */
+int sqd_op_cache_values(sqd_op_t op, void* stream);
 /* Frees the per-pair group indices of an operator with cached matrix elements (cache (1, 2)),
  * 4 bytes per stored pair; the matvec, LOCG and batching keep working, while sqd_grad_terms,
  * sqd_op_csr and sqd_op_refresh then return SQD_ERR_INVALID.  No rqutils counterpart. */

@@ -77,6 +77,7 @@ EXTRA_PROTOTYPES = {
                               _c.POINTER(_f64), _vp, _c.POINTER(_i32), _c.POINTER(_f64)]),
     'sqd_batch_destroy': (None, [_vp]),
     'sqd_op_release_groups': (_i32, [_vp]),
+    'sqd_op_cache_values': (_i32, [_vp, _vp]),
     'sqd_op_set_chunk': (_i32, [_vp, _i32, _i64]),
     'sqd_op_set_layout': (_i32, [_vp, _i32, _i32, _vp]),
     'sqd_op_get_layout': (_i32, [_vp, _i32, _c.POINTER(_i32)]),

@@ -126,7 +126,7 @@ struct CAcc {
 };
 
 // One lane's share of a CSR row: pairs i0, i0 + LPR, ... below e.  Four pairs per step with
-// independent index -> amplitude gathers in flight, then the remainder.
+// independent index -> amplitude gathers in flight, then the remainder as one predicated step.
 template <typename R, int NCV, int NCA, int LPR>
 __device__ __forceinline__ void csr_row_dot(const uint32_t* __restrict__ cols,
                                             const R* __restrict__ vals,
@@ -145,7 +145,22 @@ __device__ __forceinline__ void csr_row_dot(const uint32_t* __restrict__ cols,
     }
     acc.add4(a, x);
   }
-  for (; i < e; i += LPR) acc.add(ld_elem<R, NCA>(vals, i), ld_elem<R, NCV>(v, __ldg(cols + i)));
+  // The remainder (fewer than four pairs) as one predicated step, so its gathers are in flight
+  // together too (short rows, such as the two-half tails, are mostly remainder).  Absent pairs
+  // add exact zeros.
+  if (i < e) {
+    uint32_t c[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) c[u] = (i + u * LPR < e) ? __ldg(cols + i + u * LPR) : 0u;
+    Cx<R> a[4], x[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const bool ok = i + u * LPR < e;
+      a[u] = ok ? ld_elem<R, NCA>(vals, i + u * LPR) : cx_make<R>(R(0), R(0));
+      x[u] = ok ? ld_elem<R, NCV>(v, c[u]) : cx_make<R>(R(0), R(0));
+    }
+    acc.add4(a, x);
+  }
 }
 
 }  // namespace sqd

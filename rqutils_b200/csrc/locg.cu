@@ -128,7 +128,9 @@ __device__ void eig2(const double2 m[2][2], double* val, double2 vec[2]) {
   const double d0 = m[0][0].x, d1 = m[1][1].x;
   const double det = d0 * d1 - cabs2(m[1][0]);
   const double tr = d0 + d1;
-  const double ev = (tr - sqrt(tr * tr - 4.0 * det)) * 0.5;
+  // tr^2 - 4 det = (d0 - d1)^2 + 4 |m10|^2 >= 0; rounding can take it just below 0 for a
+  // (near-)degenerate pair, where the reference's sqrt returns NaN: clamped at 0.
+  const double ev = (tr - sqrt(fmax(tr * tr - 4.0 * det, 0.0))) * 0.5;
   const double2 num = make_double2(d1 - ev + m[1][0].x, -m[1][0].y);
   const double2 den = make_double2(d0 - ev + m[1][0].x, m[1][0].y);
   double2 v0 = cdiv(num, den);
@@ -151,12 +153,17 @@ __device__ void eig3(const double2 m[3][3], double* val, double2 vec[3]) {
   c0 -= 2.0 * cmul(cmul(m[0][2], m[1][0]), m[2][1]).x;
   const double p = c2 * c2 - 3.0 * c1;
   const double q = -13.5 * c0 - c2 * c2 * c2 + 4.5 * c2 * c1;
+  // 27 (c1^2 (p - c1) / 4 + c0 (q + 27 c0 / 4)) is 27 times the discriminant term of the
+  // characteristic cubic, >= 0 for a Hermitian matrix; rounding (and FMA contraction) can take
+  // it just below 0 for (near-)degenerate eigenvalues, where the reference's sqrt returns NaN.
+  // Clamped at 0, as are p (>= 0 likewise) below.
   const double phi =
-      atan2(sqrt(27.0 * (0.25 * c1 * c1 * (p - c1) + c0 * (q + 6.75 * c0))), q) / 3.0;
+      atan2(sqrt(fmax(27.0 * (0.25 * c1 * c1 * (p - c1) + c0 * (q + 6.75 * c0)), 0.0)), q) /
+      3.0;
   const double cphi = cos(phi), sphi = sin(phi);
   const double s3 = sqrt(3.0);
   const double xmin = fmin(fmin(2.0 * cphi, -cphi - s3 * sphi), -cphi + s3 * sphi);
-  const double ev = sqrt(p) / 3.0 * xmin - c2 / 3.0;
+  const double ev = sqrt(fmax(p, 0.0)) / 3.0 * xmin - c2 / 3.0;
   double2 a[3] = {m[0][1], m[1][1], m[2][1]};
   double2 b[3] = {m[0][2], m[1][2], m[2][2]};
   a[1].x -= ev;

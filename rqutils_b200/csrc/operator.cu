@@ -635,6 +635,23 @@ extern "C" int sqd_op_csr(sqd_op_t op, int64_t* indptr, int32_t* indices, double
   });
 }
 
+extern "C" int sqd_op_cache_values(sqd_op_t op, void* stream) {
+  return guarded([&] {
+    SQD_REQUIRE(op != nullptr, "NULL operator");
+    SQD_REQUIRE(op->x_cache == 1, "caching elements needs cached sources (cache_strategy (1, *))");
+    if (op->z_cache == 2) return;
+    op->z_cache = 2;
+    try {
+      op_values_and_lanes(op, as_stream(stream));
+    } catch (...) {
+      op->values.release();
+      op->z_cache = 0;
+      throw;
+    }
+    ++op->schedule_version;
+  });
+}
+
 extern "C" int sqd_op_release_groups(sqd_op_t op) {
   return guarded([&] {
     SQD_REQUIRE(op != nullptr, "NULL operator");

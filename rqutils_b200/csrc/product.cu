@@ -286,9 +286,20 @@ k_slab(int64_t A, int64_t B, int64_t total_k, int64_t a_tiles, const int64_t* __
       acc.add4(m + 4, xv + 4);
       vp += 8 * 32 * NCA;
     }
-    for (; k < k1; ++k) {
-      acc.add(ld_elem<R, NCA>(vp, 0), ld_elem<R, NCV>(x, int64_t(__ldg(src + k)) + b));
-      vp += 32 * NCA;
+    // remainder (fewer than eight entries): one predicated step, all gathers in flight
+    if (k < k1) {
+      uint32_t si[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) si[u] = (k + u < k1) ? __ldg(src + k + u) : 0u;
+      Cx<R> m[8], xv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const bool ok = k + u < k1;
+        m[u] = ok ? ld_elem<R, NCA>(vp, 32 * u) : cx_make<R>(R(0), R(0));
+        xv[u] = ok ? ld_elem<R, NCV>(x, int64_t(si[u]) + b) : cx_make<R>(R(0), R(0));
+      }
+      acc.add4(m, xv);
+      acc.add4(m + 4, xv + 4);
     }
     if constexpr (FINAL) st_elem<R, NCV>(out, a * B + b, cx_make<R>(acc.re.value(), acc.im.value()));
     else acc.store_partial(out_part, a * B + b);
@@ -369,13 +380,23 @@ k_slab2(int64_t A, int64_t B, int64_t total_k, int64_t a_tiles, const int64_t* _
       acc1.add4(m1, x1);
       vp += 4 * 64 * NCA;
     }
-    for (; k < k1; ++k) {
-      Cx<R> m0, m1, x0, x1;
-      pair_elem<R, NCA>(vp, m0, m1);
-      pair_vec<R, NCV, VEC>(x, int64_t(__ldg(src + k)) + b, x0, x1);
-      acc0.add(m0, x0);
-      acc1.add(m1, x1);
-      vp += 64 * NCA;
+    // remainder (fewer than four entries): one predicated step
+    if (k < k1) {
+      uint32_t si[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) si[u] = (k + u < k1) ? __ldg(src + k + u) : 0u;
+      Cx<R> m0[4], m1[4], x0[4], x1[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (k + u < k1) {
+          pair_elem<R, NCA>(vp + 64 * NCA * u, m0[u], m1[u]);
+          pair_vec<R, NCV, VEC>(x, int64_t(si[u]) + b, x0[u], x1[u]);
+        } else {
+          m0[u] = m1[u] = x0[u] = x1[u] = cx_make<R>(R(0), R(0));
+        }
+      }
+      acc0.add4(m0, x0);
+      acc1.add4(m1, x1);
     }
     if constexpr (FINAL) {
       if constexpr (VEC && NCV == 2) {

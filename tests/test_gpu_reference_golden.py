@@ -40,6 +40,10 @@ def rel(a, b):
     return np.abs(np.asarray(a) - b).max() / max(np.abs(b).max(), 1e-300)
 
 
+def host(t):
+    return t.cpu().numpy() if isinstance(t, torch.Tensor) else np.asarray(t)
+
+
 @pytest.mark.parametrize('tag,coeff_key,kw', [
     ('real_pad', 'coeffs', dict(add_padding=True)),
     ('real_nopad', 'coeffs', dict()),
@@ -62,8 +66,8 @@ def test_device_pauli_preprocessing_matches_reference(tag, coeff_key, kw):
 def test_packed_uniquify_matches_reference(tag, size):
     g = load('reference_subspace')
     su, idx = rq.uniquify_states(g['packed'], size, return_indices=True)
-    np.testing.assert_array_equal(np.asarray(su), g[f'uniq_{tag}'])
-    np.testing.assert_array_equal(np.asarray(idx), g[f'uniq_{tag}_idx'])
+    np.testing.assert_array_equal(host(su), g[f'uniq_{tag}'])
+    np.testing.assert_array_equal(host(idx), g[f'uniq_{tag}_idx'])
 
 
 @pytest.mark.parametrize('lookup', ['hash', 'bsearch'])
@@ -72,11 +76,11 @@ def test_xsource_sorted_and_unsorted_match_reference(lookup):
     su = g['uniq_plus']
     for j, x in enumerate(g['x']):
         got = rq.get_xsource(x, su, lookup=lookup)
-        np.testing.assert_array_equal(np.asarray(got), g['xsource'][j], err_msg=f'group {j}')
+        np.testing.assert_array_equal(host(got), g['xsource'][j], err_msg=f'group {j}')
     usp = np.packbits(np.pad(g['unsorted_bits'], ((0, 0), (1, 0))), axis=1)
     for j, x in enumerate(g['x']):
         got = rq.get_xsource(x, usp, sorted_input=False, lookup=lookup)
-        np.testing.assert_array_equal(np.asarray(got), g['xsource_unsorted'][j])
+        np.testing.assert_array_equal(host(got), g['xsource_unsorted'][j])
 
 
 @pytest.mark.parametrize('cache', [(1, 0), (1, 2), (0, 0), (0, 2)])
@@ -174,26 +178,28 @@ def _device_eigenpairs(mats):
 
 def test_small_eigenpairs_match_reference_and_eigh():
     """eigenpair_2x2 / eigenpair_3x3 on random, degenerate and near-degenerate Hermitian
-    matrices.  Against the reference's outputs: values to 1e-12, vectors to 1e-9 where the
-    reference's vector is finite (its cross-product vector is undefined for an exactly
-    degenerate lowest pair; the solver only meets such matrices after convergence).  Against
-    numpy.linalg.eigh: the lowest value, within 1e-12 of the spectral scale for 2x2 and
-    separated 3x3 spectra, within 1e-7 for near-degenerate ones (Cardano's method)."""
+    matrices.  Cardano's method loses about half the digits when two eigenvalues nearly meet,
+    so the bar depends on the smallest gap g of the spectrum (scale s = max |eigenvalue|):
+    g > 1e-3 s: value within 1e-12 s of the reference's and of numpy.linalg.eigh, vector within
+    1e-9 of the reference's; closer eigenvalues: value within 1e-7 s of eigh (the reference's
+    own value may be NaN there: its square roots take arguments that rounding can push below
+    zero, which the device code clamps at 0)."""
     g = load('reference_eig_small')
     for key in ('2', '3'):
         mats, vals_ref, vecs_ref = g['mats' + key], g['val' + key], g['vec' + key]
         vals, vecs = _device_eigenpairs(mats)
+        assert np.isfinite(vals).all()
         for m, val, vec, vr, ur in zip(mats, vals, vecs, vals_ref, vecs_ref):
-            scale = max(1.0, np.abs(np.linalg.eigvalsh(m)).max())
-            assert abs(val - vr) <= 1e-12 * scale
-            if np.all(np.isfinite(ur)):
-                np.testing.assert_allclose(vec, ur, rtol=0, atol=1e-9)
             w = np.linalg.eigvalsh(m)
-            gap = min(abs(w[1] - w[0]), abs(w[-1] - w[-2])) if len(w) == 3 else 1.0
-            assert abs(val - w[0]) <= (1e-12 if gap > 1e-3 else 1e-7) * scale
-            if np.all(np.isfinite(vec)) and w[1] - w[0] > 1e-3 * scale:
-                # eigenvector: residual of the lowest pair
+            scale = max(1.0, np.abs(w).max())
+            gap = np.diff(w).min()
+            if gap > 1e-3 * scale:
+                assert abs(val - vr) <= 1e-12 * scale
+                assert abs(val - w[0]) <= 1e-12 * scale
+                np.testing.assert_allclose(vec, ur, rtol=0, atol=1e-9)
                 assert np.linalg.norm(m @ vec - val * vec) <= 1e-10 * scale
+            else:
+                assert abs(val - w[0]) <= 1e-7 * scale
 
 
 def test_small_eigenpairs_reject_bad_dimensions():
@@ -237,5 +243,6 @@ def test_debug_log_level_records_and_prints_every_iteration(capsys):
     assert (np.diff(phases) <= 0).all()          # 1 ... 1 0 ... 0
     assert hist_m[-1, 5] == 1 and abs(hist_m[-1, 2] - e_m) == 0
     # no record without the debug level
+    capsys.readouterr()
     rq.ground_locg(op, op.vinit(), vspace=(op.size, torch.float64))
     assert 'LOCG iteration' not in capsys.readouterr().out

@@ -81,3 +81,25 @@ def test_mixed_precision_excited_state_with_orth():
     # the cached solver objects of an unconstrained solve are unaffected
     e_gs, _, _ = rq.ground_locg(op, x0, mode='mixed')
     assert abs(e_gs - w[0]) <= 1e-8 * abs(w[0])
+
+
+def test_promoted_element_cache_gives_the_same_results():
+    """SQDOptions.promote_cache: an operator built with the reference's default (1, 0) caches
+    its elements ((1, 2), product layout on a product subspace); Hv and the sqd energy agree
+    with the on-the-fly diagonals."""
+    wl = W.c2_small(0, 96, 80)
+    ham = rq.PauliSumXZ.from_xz(wl.x, wl.z, wl.coeffs, 32, force_real=True, padded=True)
+    space = rq.Subspace.from_u64(wl.states, 32)
+    op = rq.SQDOperator(ham, space, cache_strategy=(1, 0))
+    v = torch.as_tensor(wl.start_vector(np.complex128), device='cuda')
+    hv10 = op.matvec(v).cpu().numpy()
+    assert op.promote_cache() and op.cache_strategy == (1, 2)
+    assert op.get_layout(0) == 'product' and op.get_layout(1) == 'product'
+    hv12 = op.matvec(v).cpu().numpy()
+    assert np.abs(hv12 - hv10).max() <= 1e-13 * np.abs(hv10).max()
+    shifts = np.arange(31, -1, -1, dtype=np.uint64)
+    bits = ((wl.states[:, None] >> shifts[None, :]) & np.uint64(1)).astype(np.uint8)
+    e_on = rq.sqd((wl.labels, list(wl.coeffs)), bits, options={'promote_cache': False,
+                                                                'return_eigvec': False})
+    e_pr = rq.sqd((wl.labels, list(wl.coeffs)), bits, options={'return_eigvec': False})
+    assert abs(e_on - e_pr) <= 1e-12 * abs(e_on)
