@@ -89,17 +89,22 @@ def load_peaks():
     return 6650.0, 'fallback'
 
 
+# Sources of the matvec kernels (and the headers they include): the traffic of a committed
+# profile summary is used only while these are unchanged.
+MATVEC_SOURCES = ('accum.cuh', 'common.cuh', 'dispatch.cuh', 'internal.cuh', 'matvec.cu',
+                  'product.cu', 'sweep.cuh')
+
+
 def kernel_sources_digest():
-    """SHA-256 over the CUDA sources (name and bytes, sorted by name): identifies the kernels
-    a profile summary was captured on."""
+    """SHA-256 over the matvec kernels' sources (name and bytes, sorted by name): identifies
+    the kernels a profile summary was captured on."""
     import hashlib
     csrc = os.path.join(ROOT, 'rqutils_b200', 'csrc')
     h = hashlib.sha256()
-    for name in sorted(os.listdir(csrc)):
-        if name.endswith(('.cu', '.cuh', '.h')):
-            h.update(name.encode())
-            with open(os.path.join(csrc, name), 'rb') as f:
-                h.update(f.read())
+    for name in sorted(MATVEC_SOURCES):
+        h.update(name.encode())
+        with open(os.path.join(csrc, name), 'rb') as f:
+            h.update(f.read())
     return h.hexdigest()
 
 

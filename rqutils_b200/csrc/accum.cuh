@@ -127,7 +127,8 @@ struct CAcc {
 
 // One lane's share of a CSR row: pairs i0, i0 + LPR, ... below e.  Four pairs per step with
 // independent index -> amplitude gathers in flight, then the remainder as one predicated step.
-template <typename R, int NCV, int NCA, int LPR>
+// CG: read v through L2 (v written earlier in the same launch by other blocks).
+template <typename R, int NCV, int NCA, int LPR, bool CG = false>
 __device__ __forceinline__ void csr_row_dot(const uint32_t* __restrict__ cols,
                                             const R* __restrict__ vals,
                                             const R* __restrict__ v, int64_t i0, int64_t e,
@@ -141,7 +142,7 @@ __device__ __forceinline__ void csr_row_dot(const uint32_t* __restrict__ cols,
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       a[u] = ld_elem<R, NCA>(vals, i + u * LPR);
-      x[u] = ld_elem<R, NCV>(v, c[u]);
+      x[u] = CG ? ld_elem_cg<R, NCV>(v, c[u]) : ld_elem<R, NCV>(v, c[u]);
     }
     acc.add4(a, x);
   }
@@ -157,7 +158,8 @@ __device__ __forceinline__ void csr_row_dot(const uint32_t* __restrict__ cols,
     for (int u = 0; u < 4; ++u) {
       const bool ok = i + u * LPR < e;
       a[u] = ok ? ld_elem<R, NCA>(vals, i + u * LPR) : cx_make<R>(R(0), R(0));
-      x[u] = ok ? ld_elem<R, NCV>(v, c[u]) : cx_make<R>(R(0), R(0));
+      x[u] = ok ? (CG ? ld_elem_cg<R, NCV>(v, c[u]) : ld_elem<R, NCV>(v, c[u]))
+                : cx_make<R>(R(0), R(0));
     }
     acc.add4(a, x);
   }

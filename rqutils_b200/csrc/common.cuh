@@ -158,6 +158,23 @@ __device__ __forceinline__ Cx<R> ld_elem(const R* p, int64_t i) {
 }
 
 // Plain (coherent) load, for buffers written earlier in the same kernel sequence on-device.
+// Load through L2 only (ld.global.cg): for data written earlier in the same kernel launch by
+// other thread blocks, which a non-coherent L1 copy could shadow.
+template <typename R, int NC>
+__device__ __forceinline__ Cx<R> ld_elem_cg(const R* p, int64_t i) {
+  if constexpr (NC == 2) {
+    if constexpr (sizeof(R) == 8) {
+      const double2 v = __ldcg(reinterpret_cast<const double2*>(p) + i);
+      return cx_make<R>(v.x, v.y);
+    } else {
+      const float2 v = __ldcg(reinterpret_cast<const float2*>(p) + i);
+      return cx_make<R>(v.x, v.y);
+    }
+  } else {
+    return cx_make<R>(__ldcg(p + i), R(0));
+  }
+}
+
 template <typename R, int NC>
 __device__ __forceinline__ Cx<R> ld_elem_rw(const R* p, int64_t i) {
   if constexpr (NC == 2) {

@@ -84,6 +84,8 @@ struct LocgDev {
   int hist_phase;        // first column of every row: 0 = FP64 iteration, 1 = FP32 sweep
 };
 
+static_assert(sizeof(LocgDev) % sizeof(long long) == 0, "LocgDev is copied in 8-byte words");
+
 // Columns of a history row: phase, iteration, theta, |r|, reltol ((|Ax| - theta) * 10 N; the
 // FP32 sweeps store their stopping threshold inner_rtol * |theta| there), converged.
 constexpr int kHistCols = 6;
@@ -755,6 +757,211 @@ __global__ void k_convert(const RI* in, RO* out, int64_t n) {
   }
 }
 
+// ------------------------------------------------------------- persistent implicit iteration
+// The fast implicit iteration (5 fused passes + 1 cached CSR matvec) as ONE cooperative launch
+// that loops until the convergence step sets `done`.  On small operators the graph form is
+// bound by its ~6 dependent launches per iteration, each a few microseconds of launch and
+// drain; here the phases are separated by a grid barrier instead.  The last block to reach a
+// barrier sums the dot partials of all blocks (fixed order) before it releases the others;
+// every block then runs the scalar step on its own shared-memory copy of the solver state from
+// the same sums, so all blocks hold bit-identical coefficients without a second barrier;
+// block 0 writes the history rows and, at the end, the state back.
+// Vectors written within the launch are read through L2 (ld.global.cg).
+struct PersistArgs {
+  LCArgs<6, 10, 5> ps[5];      // body_fast's passes in order (the matvec follows ps[1])
+  const int64_t* row_ptr;      // cached CSR operator
+  const uint32_t* cols;
+  const void* vals;            // FP64 or FP32 elements, as the vectors
+  const void* mv_in;           // p
+  void* mv_out;                // A p
+  int64_t n;
+  LocgDev* dev;
+  double* partials;            // gridDim.x x 20 doubles: per-block dot partials
+  double* red;                 // 20 doubles: the sums, from the last block of a barrier
+  unsigned* bar;               // [0] arrivals, [1] generation, [2] fault (zeroed per launch)
+  int max_iter;
+};
+
+constexpr long long kBarrierSpinLimit = 1ll << 25;   // most with >= 64 ns sleeps: > 2 s
+
+// Grid barrier for a cooperative launch (all blocks co-resident).  Bounded: a block that
+// waits too long, or sees another block's fault, records the fault and returns false, and the
+// kernel returns; the host reports it.  When `part` is given, the last block to arrive sums the
+// nv per-block partials (in block order, as final_reduce does) into red_g before it releases
+// the others, which then read the nv sums; the sums end up in sd.red in every block.
+__device__ __forceinline__ bool persist_barrier(unsigned* bar, unsigned& gen,
+                                                const double* part = nullptr, int nv = 0,
+                                                double* red_g = nullptr, LocgDev* sd = nullptr) {
+  __shared__ int last_s, ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last_s = gridDim.x == 1 || atomicAdd(&bar[0], 1u) == gridDim.x - 1;
+    ok_s = 1;
+  }
+  __syncthreads();
+  if (last_s) {
+    if (part != nullptr) {
+      final_reduce<20>(part, nv, sd);
+      __syncthreads();
+      if (threadIdx.x < nv) red_g[threadIdx.x] = sd->red[threadIdx.x >> 1][threadIdx.x & 1];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && gridDim.x > 1) {
+      atomicExch(&bar[0], 0u);
+      __threadfence();
+      atomicAdd(&bar[1], 1u);
+    }
+  } else if (threadIdx.x == 0) {
+    long long spins = 0;
+    while (*reinterpret_cast<volatile unsigned*>(&bar[1]) == gen) {
+      if (*reinterpret_cast<volatile unsigned*>(&bar[2]) != 0u || ++spins > kBarrierSpinLimit) {
+        atomicExch(&bar[2], 1u);
+        ok_s = 0;
+        break;
+      }
+      if (spins > 4096) __nanosleep(64);   // poll back to back first: most waits are short
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  ++gen;
+  if (!ok_s) return false;
+  if (part != nullptr && !last_s) {
+    if (threadIdx.x < nv) sd->red[threadIdx.x >> 1][threadIdx.x & 1] = __ldcg(red_g + threadIdx.x);
+    __syncthreads();
+  }
+  return true;
+}
+
+template <typename R, int NC, typename S>
+__device__ __forceinline__ bool persist_pass(const LCArgs<6, 10, 5>& a, LocgDev& sd,
+                                             const PersistArgs& pa, unsigned& gen) {
+  constexpr int NS = S::NS, NO = S::NO, ND = S::ND;
+  constexpr int NOA = NO > 0 ? NO : 1, NDA = ND > 0 ? ND : 1;
+  double acc[NDA][2];
+#pragma unroll
+  for (int d = 0; d < NDA; ++d) acc[d][0] = acc[d][1] = 0.0;
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  constexpr int64_t EB = int64_t(sizeof(R)) * NC;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < a.n; i += stride) {
+    double2 sv[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      const Cx<R> v = ld_elem_cg<R, NC>(static_cast<const R*>(a.src[k]), i);
+      sv[k] = make_double2(double(v.re), double(v.im));
+    }
+    if (i + stride < a.n) {
+#pragma unroll
+      for (int k = 0; k < NS; ++k)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(static_cast<const char*>(a.src[k]) +
+                                                       (i + stride) * EB));
+    }
+    double2 ov[NOA];
+#pragma unroll
+    for (int q = 0; q < NO; ++q) {
+      double2 t = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < NS; ++k)
+        t = cadd(t, cmul(make_double2(sd.coef[q][k][0], sd.coef[q][k][1]), sv[k]));
+      if constexpr (NC == 1) t.y = 0.0;
+      ov[q] = t;
+    }
+    DotLoop<S, 0, ND>::run(acc, sv, ov);
+#pragma unroll
+    for (int q = 0; q < NO; ++q)
+      if (a.out[q] != nullptr)
+        st_elem<R, NC>(static_cast<R*>(a.out[q]), i, cx_make<R>(R(ov[q].x), R(ov[q].y)));
+  }
+  double* part = pa.partials;
+  if constexpr (ND > 0) {
+    __shared__ double sred[NDA * 2][LC_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const double v0 = warp_sum(acc[d][0]);
+      const double v1 = warp_sum(acc[d][1]);
+      if (lane == 0) {
+        sred[2 * d][warp] = v0;
+        sred[2 * d + 1][warp] = v1;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * ND) {
+      double t = 0.0;
+      for (int w = 0; w < LC_THREADS / 32; ++w) t += sred[threadIdx.x][w];
+      part[static_cast<int64_t>(blockIdx.x) * 20 + threadIdx.x] = t;
+    }
+  }
+  if constexpr (ND > 0) {
+    if (!persist_barrier(pa.bar, gen, part, 2 * ND, pa.red, &sd)) return false;
+  } else {
+    if (!persist_barrier(pa.bar, gen)) return false;
+  }
+  if (threadIdx.x == 0 && a.post != P_NONE) run_post(&sd, a.post, a.nsrc, 0, 0);
+  __syncthreads();
+  return true;
+}
+
+template <typename R, int NCV, int NCA, int LPR>
+__device__ __forceinline__ void persist_matvec(const PersistArgs& pa) {
+  constexpr int RPW = 32 / LPR;
+  const int lane = threadIdx.x & 31;
+  const int sub = lane % LPR, slot = lane / LPR;
+  const R* vals = static_cast<const R*>(pa.vals);
+  const R* v = static_cast<const R*>(pa.mv_in);
+  R* out = static_cast<R*>(pa.mv_out);
+  const int64_t w0 = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t rb = w0 * RPW; rb < pa.n; rb += nw * RPW) {
+    const int64_t row = rb + slot;
+    CAcc<R, NCV, NCA> acc;
+    if (row < pa.n) {
+      const int64_t b = __ldg(pa.row_ptr + row), e = __ldg(pa.row_ptr + row + 1);
+      csr_row_dot<R, NCV, NCA, LPR, true>(pa.cols, vals, v, b + sub, e, acc);
+    }
+    acc.merge(LPR);
+    if (sub == 0 && row < pa.n)
+      st_elem<R, NCV>(out, row, cx_make<R>(acc.re.value(), acc.im.value()));
+  }
+}
+
+using PShape0 = PassShape<3, 1, 100, 100, 1, 100, 2, 100>;
+using PShape1 = PassShape<3, 1>;
+using PShape2 = PassShape<6, 0, 0, 3, 1, 4, 2, 5, 1, 3, 2, 3, 2, 4, 2, 2, 1, 2>;
+using PShape3 = PassShape<6, 4, 100, 100, 101, 101>;
+using PShape4 = PassShape<4, 5, 104, 104, 102, 102, 100, 104, 101, 104>;
+
+template <typename R, int NC, int NCA, int LPR>
+__global__ void __launch_bounds__(LC_THREADS, 3) k_locg_persist(PersistArgs pa) {
+  __shared__ LocgDev sd;
+  {
+    const long long* src = reinterpret_cast<const long long*>(pa.dev);
+    long long* dst = reinterpret_cast<long long*>(&sd);
+    for (int i = threadIdx.x; i < int(sizeof(LocgDev) / sizeof(long long)); i += blockDim.x)
+      dst[i] = __ldcg(src + i);
+  }
+  __syncthreads();
+  if (blockIdx.x != 0 && threadIdx.x == 0) sd.hist = nullptr;   // block 0 records
+  __syncthreads();
+  unsigned gen = 0;
+  for (int it = 0; it < pa.max_iter && !sd.done; ++it) {
+    if (!persist_pass<R, NC, PShape0>(pa.ps[0], sd, pa, gen)) return;
+    if (!persist_pass<R, NC, PShape1>(pa.ps[1], sd, pa, gen)) return;
+    persist_matvec<R, NC, NCA, LPR>(pa);
+    if (!persist_barrier(pa.bar, gen)) return;
+    if (!persist_pass<R, NC, PShape2>(pa.ps[2], sd, pa, gen)) return;
+    if (!persist_pass<R, NC, PShape3>(pa.ps[3], sd, pa, gen)) return;
+    if (!persist_pass<R, NC, PShape4>(pa.ps[4], sd, pa, gen)) return;
+  }
+  if (blockIdx.x == 0) {
+    const long long* src = reinterpret_cast<const long long*>(&sd);
+    long long* dst = reinterpret_cast<long long*>(pa.dev);
+    for (int i = threadIdx.x; i < int(sizeof(LocgDev) / sizeof(long long)); i += blockDim.x)
+      dst[i] = src[i];
+  }
+}
+
 // ----------------------------------------------------------------------------- host driver
 struct Vec {
   void* p = nullptr;
@@ -1033,6 +1240,10 @@ class Locg {
             bool fast = false) {
     read_host();
     if (maxiter <= 0 || host_->done) return;
+    if (fast && use_graph && orth.empty() && persist_op_ != nullptr) {
+      loop_persistent(maxiter);
+      return;
+    }
     auto run_body = [&] {
       if (fast) body_fast(orth);
       else body(orth);
@@ -1152,6 +1363,77 @@ class Locg {
     return m ? m : "";
   }
 
+ public:
+  // The fast iteration may run as one persistent launch (k_locg_persist) when the matvec is
+  // this cached operator's CSR kernel; nullptr keeps the graph form.
+  void set_persistent_op(sqd_op_s* op) { persist_op_ = op; }
+
+ private:
+  template <int NCA, int LPR>
+  void launch_persistent(PersistArgs& pa) {
+    auto kern = k_locg_persist<R, NC, NCA, LPR>;
+    if (persist_grid_ == 0) {
+      int per_sm = 0;
+      SQD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, LC_THREADS, 0));
+      const int64_t want = (n_ + LC_THREADS - 1) / LC_THREADS;
+      const int64_t cap = static_cast<int64_t>(std::max(per_sm, 1)) * num_sms();
+      persist_grid_ = static_cast<unsigned>(std::max<int64_t>(1, std::min(want, cap)));
+      ppart_.alloc(static_cast<size_t>(persist_grid_) * 20 + 20, st_);
+      bar_.alloc(4, st_);
+    }
+    pa.partials = ppart_.ptr;
+    pa.red = ppart_.ptr + static_cast<size_t>(persist_grid_) * 20;
+    pa.bar = bar_.ptr;
+    SQD_CUDA(cudaMemsetAsync(bar_.ptr, 0, 4 * sizeof(unsigned), st_));
+    void* args[] = {&pa};
+    SQD_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kern), persist_grid_,
+                                         LC_THREADS, args, 0, st_));
+  }
+
+  // loop(fast) as one cooperative launch: the body_fast passes and the CSR matvec, phases
+  // separated by grid barriers, until the convergence step sets `done`.
+  void loop_persistent(int maxiter) {
+    sqd_op_s* op = persist_op_;
+    R *x = x_.ptr, *y = y_.ptr, *r = r_.ptr, *p = p_.ptr;
+    R *ax = ax_.ptr, *ay = ay_.ptr, *ap = ap_.ptr;
+    PersistArgs pa{};
+    fill(pa.ps[0], {r, x, y}, {p}, {{100, 100}, {1, 100}, {2, 100}}, P_PROJ_NORM_IPS, G_NONE);
+    fill(pa.ps[1], {p, x, y}, {p}, {}, P_NONE, G_NONE);
+    fill(pa.ps[2], {x, y, p, ax, ay, ap}, {},
+         {{0, 3}, {1, 4}, {2, 5}, {1, 3}, {2, 3}, {2, 4}, {2, 2}, {1, 2}}, P_GRAM_IMPLICIT,
+         G_NONE);
+    fill(pa.ps[3], {x, y, p, ax, ay, ap}, {x, y, ax, ay}, {{100, 100}, {101, 101}},
+         P_UPDATE_NORMS, G_NONE);
+    fill(pa.ps[4], {x, y, ax, ay}, {x, y, ax, ay, r},
+         {{104, 104}, {102, 102}, {100, 104}, {101, 104}}, P_CONV_PROJ, G_NONE);
+    pa.row_ptr = op->row_ptr.ptr;
+    pa.cols = op->cols.ptr;
+    if constexpr (sizeof(R) == 8) pa.vals = op->values.ptr;
+    else pa.vals = op->values32.ptr;
+    pa.mv_in = p;
+    pa.mv_out = ap;
+    pa.n = n_;
+    pa.dev = dev_.ptr;
+    pa.max_iter = maxiter + 1;
+    const int lpr = op->lanes_per_row[sizeof(R) == 8 ? 0 : 1];
+    dispatch_lpr(lpr, [&](auto lpr_t) {
+      constexpr int LPR = decltype(lpr_t)::value;
+      if constexpr (NC == 2) {
+        if (op->value_complex) launch_persistent<2, LPR>(pa);
+        else launch_persistent<1, LPR>(pa);
+      } else {
+        launch_persistent<1, LPR>(pa);
+      }
+    });
+    read_host();
+    unsigned fault = 0;
+    SQD_CUDA(cudaMemcpyAsync(&fault, bar_.ptr + 2, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                             st_));
+    SQD_CUDA(cudaStreamSynchronize(st_));
+    if (fault)
+      throw Error(SQD_ERR_DEVICE, "persistent LOCG iteration: a grid barrier timed out");
+  }
+
   int64_t n_;
   sqd_matvec_fn fn_;
   void* ctx_;
@@ -1160,6 +1442,10 @@ class Locg {
   double* hist_ = nullptr;
   int hist_cap_ = 0;
   int hist_phase_ = 0;
+  sqd_op_s* persist_op_ = nullptr;
+  unsigned persist_grid_ = 0;
+  DevBuf<double> ppart_;
+  DevBuf<unsigned> bar_;
   unsigned blocks_ = 1;
   DevBuf<double> partials_;
   DevBuf<unsigned> counter_;
@@ -1370,6 +1656,19 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, sqd_op_s* cache
   // always set: a cached solver must not keep a previous solve's (freed) record buffer
   L.set_history(rec.rows[0].ptr, static_cast<int>(rec.req.max_rows), 0);
   l32->set_history(rec.rows[1].ptr, static_cast<int>(rec.req.max_rows), 1);
+  // Persistent iterations (one cooperative launch per loop) where the matvec is the cached
+  // CSR kernel and the operator is small enough that launch latency, not bandwidth, bounds the
+  // graph form (up to 4 Mi rows; SQD_LOCG_PERSISTENT=0 disables, =1 forces).
+  {
+    const char* env = std::getenv("SQD_LOCG_PERSISTENT");
+    const bool on = env ? std::atoi(env) != 0 : n <= (int64_t(4) << 20);
+    auto csr = [&](int prec) {
+      return op->x_cache == 1 && op->z_cache == 2 &&
+             (!op->prod.built || op->layout[prec] == SQD_LAYOUT_CSR);
+    };
+    l32->set_persistent_op(on && csr(1) ? op : nullptr);
+    L.set_persistent_op(on && csr(0) ? op : nullptr);
+  }
   {
     Locg<float, NC>& L32 = *l32;
     L32.set_stream(st);
