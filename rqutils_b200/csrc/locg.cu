@@ -14,6 +14,7 @@
 // Inner products always accumulate in FP64 (also for FP32 vectors).
 #include <cstdio>
 #include <cstdlib>
+#include <cooperative_groups.h>
 
 #include "internal.cuh"
 #include "dispatch.cuh"
@@ -834,9 +835,26 @@ __device__ __forceinline__ bool persist_barrier(unsigned* bar, unsigned& gen,
   return true;
 }
 
-template <typename R, int NC, typename S>
+// Sync of all blocks at the end of a phase.  CLU (the grid is one thread-block cluster): the
+// hardware cluster barrier (release/acquire at cluster scope); otherwise the bounded grid
+// barrier above.
+template <bool CLU>
+__device__ __forceinline__ bool persist_sync(const PersistArgs& pa, unsigned& gen) {
+  if constexpr (CLU) {
+    __threadfence();
+    cooperative_groups::this_cluster().sync();
+    return true;
+  } else {
+    return persist_barrier(pa.bar, gen);
+  }
+}
+
+// cpart (CLU only): the kernel's shared [2][20] partials, alternating per dot pass; every block
+// sums the blocks' partials through distributed shared memory in rank order.
+template <typename R, int NC, typename S, bool CLU>
 __device__ __forceinline__ bool persist_pass(const LCArgs<6, 10, 5>& a, LocgDev& sd,
-                                             const PersistArgs& pa, unsigned& gen) {
+                                             const PersistArgs& pa, unsigned& gen,
+                                             double* cpart, int& buf) {
   constexpr int NS = S::NS, NO = S::NO, ND = S::ND;
   constexpr int NOA = NO > 0 ? NO : 1, NDA = ND > 0 ? ND : 1;
   double acc[NDA][2];
@@ -890,10 +908,24 @@ __device__ __forceinline__ bool persist_pass(const LCArgs<6, 10, 5>& a, LocgDev&
     if (threadIdx.x < 2 * ND) {
       double t = 0.0;
       for (int w = 0; w < LC_THREADS / 32; ++w) t += sred[threadIdx.x][w];
-      part[static_cast<int64_t>(blockIdx.x) * 20 + threadIdx.x] = t;
+      if constexpr (CLU) cpart[buf * 20 + threadIdx.x] = t;
+      else part[static_cast<int64_t>(blockIdx.x) * 20 + threadIdx.x] = t;
     }
   }
-  if constexpr (ND > 0) {
+  if constexpr (CLU) {
+    persist_sync<true>(pa, gen);
+    if constexpr (ND > 0) {
+      if (threadIdx.x < 2 * ND) {
+        cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+        double v = 0.0;
+        for (unsigned b = 0; b < cl.num_blocks(); ++b)
+          v += cl.map_shared_rank(cpart + buf * 20, b)[threadIdx.x];
+        sd.red[threadIdx.x >> 1][threadIdx.x & 1] = v;
+      }
+      buf ^= 1;
+      __syncthreads();
+    }
+  } else if constexpr (ND > 0) {
     if (!persist_barrier(pa.bar, gen, part, 2 * ND, pa.red, &sd)) return false;
   } else {
     if (!persist_barrier(pa.bar, gen)) return false;
@@ -932,9 +964,10 @@ using PShape2 = PassShape<6, 0, 0, 3, 1, 4, 2, 5, 1, 3, 2, 3, 2, 4, 2, 2, 1, 2>;
 using PShape3 = PassShape<6, 4, 100, 100, 101, 101>;
 using PShape4 = PassShape<4, 5, 104, 104, 102, 102, 100, 104, 101, 104>;
 
-template <typename R, int NC, int NCA, int LPR>
+template <typename R, int NC, int NCA, int LPR, bool CLU>
 __global__ void __launch_bounds__(LC_THREADS, 3) k_locg_persist(PersistArgs pa) {
   __shared__ LocgDev sd;
+  __shared__ double cpart[2 * 20];
   {
     const long long* src = reinterpret_cast<const long long*>(pa.dev);
     long long* dst = reinterpret_cast<long long*>(&sd);
@@ -945,15 +978,17 @@ __global__ void __launch_bounds__(LC_THREADS, 3) k_locg_persist(PersistArgs pa) 
   if (blockIdx.x != 0 && threadIdx.x == 0) sd.hist = nullptr;   // block 0 records
   __syncthreads();
   unsigned gen = 0;
+  int buf = 0;
   for (int it = 0; it < pa.max_iter && !sd.done; ++it) {
-    if (!persist_pass<R, NC, PShape0>(pa.ps[0], sd, pa, gen)) return;
-    if (!persist_pass<R, NC, PShape1>(pa.ps[1], sd, pa, gen)) return;
+    if (!persist_pass<R, NC, PShape0, CLU>(pa.ps[0], sd, pa, gen, cpart, buf)) return;
+    if (!persist_pass<R, NC, PShape1, CLU>(pa.ps[1], sd, pa, gen, cpart, buf)) return;
     persist_matvec<R, NC, NCA, LPR>(pa);
-    if (!persist_barrier(pa.bar, gen)) return;
-    if (!persist_pass<R, NC, PShape2>(pa.ps[2], sd, pa, gen)) return;
-    if (!persist_pass<R, NC, PShape3>(pa.ps[3], sd, pa, gen)) return;
-    if (!persist_pass<R, NC, PShape4>(pa.ps[4], sd, pa, gen)) return;
+    if (!persist_sync<CLU>(pa, gen)) return;
+    if (!persist_pass<R, NC, PShape2, CLU>(pa.ps[2], sd, pa, gen, cpart, buf)) return;
+    if (!persist_pass<R, NC, PShape3, CLU>(pa.ps[3], sd, pa, gen, cpart, buf)) return;
+    if (!persist_pass<R, NC, PShape4, CLU>(pa.ps[4], sd, pa, gen, cpart, buf)) return;
   }
+  if constexpr (CLU) persist_sync<true>(pa, gen);   // no block leaves while others read its smem
   if (blockIdx.x == 0) {
     const long long* src = reinterpret_cast<const long long*>(&sd);
     long long* dst = reinterpret_cast<long long*>(pa.dev);
@@ -1369,15 +1404,25 @@ class Locg {
   void set_persistent_op(sqd_op_s* op) { persist_op_ = op; }
 
  private:
+  // Small vectors (at most kClusterMax blocks' worth): the grid is one thread-block cluster,
+  // synchronised by the hardware cluster barrier with the partials exchanged through
+  // distributed shared memory.  Larger: a cooperative launch with the bounded grid barrier.
+  static constexpr int kClusterMax = 16;
+
   template <int NCA, int LPR>
   void launch_persistent(PersistArgs& pa) {
-    auto kern = k_locg_persist<R, NC, NCA, LPR>;
+    const int64_t want = (n_ + LC_THREADS - 1) / LC_THREADS;
     if (persist_grid_ == 0) {
-      int per_sm = 0;
-      SQD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, LC_THREADS, 0));
-      const int64_t want = (n_ + LC_THREADS - 1) / LC_THREADS;
-      const int64_t cap = static_cast<int64_t>(std::max(per_sm, 1)) * num_sms();
-      persist_grid_ = static_cast<unsigned>(std::max<int64_t>(1, std::min(want, cap)));
+      if (want <= kClusterMax) {
+        persist_cluster_ = true;
+        persist_grid_ = static_cast<unsigned>(std::max<int64_t>(1, want));
+      } else {
+        int per_sm = 0;
+        SQD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, k_locg_persist<R, NC, NCA, LPR, false>, LC_THREADS, 0));
+        const int64_t cap = static_cast<int64_t>(std::max(per_sm, 1)) * num_sms();
+        persist_grid_ = static_cast<unsigned>(std::max<int64_t>(1, std::min(want, cap)));
+      }
       ppart_.alloc(static_cast<size_t>(persist_grid_) * 20 + 20, st_);
       bar_.alloc(4, st_);
     }
@@ -1385,9 +1430,28 @@ class Locg {
     pa.red = ppart_.ptr + static_cast<size_t>(persist_grid_) * 20;
     pa.bar = bar_.ptr;
     SQD_CUDA(cudaMemsetAsync(bar_.ptr, 0, 4 * sizeof(unsigned), st_));
-    void* args[] = {&pa};
-    SQD_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kern), persist_grid_,
-                                         LC_THREADS, args, 0, st_));
+    if (persist_cluster_) {
+      auto kern = k_locg_persist<R, NC, NCA, LPR, true>;
+      if (persist_grid_ > 8)
+        SQD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3(persist_grid_);
+      cfg.blockDim = dim3(LC_THREADS);
+      cfg.stream = st_;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = persist_grid_;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      SQD_CUDA(cudaLaunchKernelEx(&cfg, kern, pa));
+    } else {
+      auto kern = k_locg_persist<R, NC, NCA, LPR, false>;
+      void* args[] = {&pa};
+      SQD_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kern), persist_grid_,
+                                           LC_THREADS, args, 0, st_));
+    }
   }
 
   // loop(fast) as one cooperative launch: the body_fast passes and the CSR matvec, phases
@@ -1444,6 +1508,7 @@ class Locg {
   int hist_phase_ = 0;
   sqd_op_s* persist_op_ = nullptr;
   unsigned persist_grid_ = 0;
+  bool persist_cluster_ = false;
   DevBuf<double> ppart_;
   DevBuf<unsigned> bar_;
   unsigned blocks_ = 1;
