@@ -1420,6 +1420,8 @@ class Locg {
         int per_sm = 0;
         SQD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
             &per_sm, k_locg_persist<R, NC, NCA, LPR, false>, LC_THREADS, 0));
+        if (const char* e = std::getenv("SQD_LOCG_PERSIST_BLOCKS"))   // per SM (tuning)
+          per_sm = std::min(per_sm, std::max(1, std::atoi(e)));
         const int64_t cap = static_cast<int64_t>(std::max(per_sm, 1)) * num_sms();
         persist_grid_ = static_cast<unsigned>(std::max<int64_t>(1, std::min(want, cap)));
       }
@@ -1723,10 +1725,12 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, sqd_op_s* cache
   l32->set_history(rec.rows[1].ptr, static_cast<int>(rec.req.max_rows), 1);
   // Persistent iterations (one cooperative launch per loop) where the matvec is the cached
   // CSR kernel and the operator is small enough that launch latency, not bandwidth, bounds the
-  // graph form (up to 4 Mi rows; SQD_LOCG_PERSISTENT=0 disables, =1 forces).
+  // graph form: up to 4 Mi rows and 64 Mi stored pairs (a large matvec runs better as its own
+  // kernel at full occupancy).  SQD_LOCG_PERSISTENT=0 disables, =1 forces.
   {
     const char* env = std::getenv("SQD_LOCG_PERSISTENT");
-    const bool on = env ? std::atoi(env) != 0 : n <= (int64_t(4) << 20);
+    const bool on = env ? std::atoi(env) != 0
+                        : n <= (int64_t(4) << 20) && op->nnz <= (int64_t(64) << 20);
     auto csr = [&](int prec) {
       return op->x_cache == 1 && op->z_cache == 2 &&
              (!op->prod.built || op->layout[prec] == SQD_LAYOUT_CSR);
