@@ -112,3 +112,32 @@ class CpuMatvecSample:
         for p in self.pools:
             p.terminate()
             p.join()
+
+
+def projected_csr(x, z, coeffs, states):
+    """The projected Hamiltonian <i|H|j> on sorted unique uint64 ``states`` as a SciPy CSR
+    matrix (what ``hproj`` returns, sqd.py:269-314, with the states padded consistently): per X
+    group, the sources by a sorted search (get_xsource's result for sorted unique rows) and the
+    composed diagonal of get_diagonal (sqd.py:603-628) at the rows whose source exists."""
+    import scipy.sparse as sps
+    gx, gstart, zt, c = group_terms(x, z, coeffs)
+    s = np.asarray(states, dtype=np.uint64)
+    n = s.shape[0]
+    rows, cols, data = [], [], []
+    for j in range(gx.shape[0]):
+        t = s ^ gx[j]
+        pos = np.minimum(np.searchsorted(s, t), n - 1)
+        ok = s[pos] == t
+        if not ok.any():
+            continue
+        r = np.nonzero(ok)[0]
+        diag = np.zeros(r.shape[0], dtype=c.dtype)
+        for k in range(gstart[j], gstart[j + 1]):
+            if c[k] == 0:
+                break
+            diag = diag + c[k] * (1. - 2. * (np.bitwise_count(s[r] & zt[k]) & 1))
+        rows.append(r)
+        cols.append(pos[r])
+        data.append(diag)
+    return sps.csr_matrix((np.concatenate(data), (np.concatenate(rows), np.concatenate(cols))),
+                          shape=(n, n))

@@ -1,5 +1,6 @@
 """Batched instances: the batched mixed-precision solver agrees per instance with the
-single-instance FP64 solver (1e-8 relative) and with dense eigh where the subspace is small."""
+single-instance FP64 solver (1e-8 relative), with the lowest eigenvalue of the oracle's sparse
+projected matrix for every instance, and with dense eigh where the subspace is small."""
 import numpy as np
 import pytest
 import torch
@@ -8,6 +9,7 @@ import rqutils_b200 as rq
 from rqutils_b200 import workloads as W
 from rqutils_b200.batched import SQDBatch, solve_instances
 from oracle import dense as OD
+from oracle.cpu_baseline import projected_csr
 
 pytestmark = pytest.mark.gpu
 
@@ -55,3 +57,14 @@ def test_wave_scheduler_splits_by_budget(instances):
     e_alone, _ = solve_instances(instances, alone_pairs=0)          # every instance alone
     np.testing.assert_allclose(e_waves, e_all, rtol=1e-8)
     np.testing.assert_allclose(e_alone, e_all, rtol=1e-8)
+
+
+def test_batched_every_instance_against_the_oracle_matrix(instances):
+    """Each instance's batched energy against the lowest eigenvalue of the oracle's projected
+    sparse matrix (ARPACK, 1e-12 tolerance), 1e-8 relative."""
+    from scipy.sparse.linalg import eigsh
+    e, _ = solve_instances(instances)
+    for k, w in enumerate(instances):
+        h = projected_csr(w.x, w.z, w.coeffs, w.states)
+        e0 = eigsh(h, k=1, which='SA', tol=1e-12)[0][0]
+        assert abs(e[k] - e0) <= 1e-8 * abs(e0), (k, e[k], e0)

@@ -51,3 +51,15 @@ def test_real_hamiltonians_match_the_reference_matvec(tag):
     hv = _sample_matvec(x, z, g[f'{tag}_coeffs'], states, np.arange(states.shape[0]),
                         g[f'{tag}_probes'][0])
     assert rel(hv, g[f'{tag}_hv'][0]) < SUM_RTOL
+
+
+@pytest.mark.parametrize('tag', ['evy12', 'jw8'])
+def test_projected_csr_matches_the_reference_matvec(tag):
+    from oracle.cpu_baseline import projected_csr
+    g = load('reference_solves')
+    lab = [s.decode() for s in g[f'{tag}_labels']]
+    x, z, n = W.xz_from_labels(lab)
+    states = np.unique(OQ.states_to_u64(g[f'{tag}_bits']))
+    h = projected_csr(x, z, g[f'{tag}_coeffs'], states)
+    assert rel(h @ g[f'{tag}_probes'][0], g[f'{tag}_hv'][0]) < SUM_RTOL
+    assert abs(h - h.conj().T).max() == 0
