@@ -1481,7 +1481,10 @@ class Locg {
     pa.n = n_;
     pa.dev = dev_.ptr;
     pa.max_iter = maxiter + 1;
-    const int lpr = op->lanes_per_row[sizeof(R) == 8 ? 0 : 1];
+    // Lanes per row from the mean row length, not the standalone matvec's tuned value: inside
+    // the persistent launch the grid is small and a row's lanes should not exceed its pairs.
+    const double avg = n_ > 0 ? static_cast<double>(op->nnz) / static_cast<double>(n_) : 0.0;
+    const int lpr = avg >= 96 ? 32 : avg >= 40 ? 16 : avg >= 16 ? 8 : avg >= 6 ? 4 : 2;
     dispatch_lpr(lpr, [&](auto lpr_t) {
       constexpr int LPR = decltype(lpr_t)::value;
       if constexpr (NC == 2) {
