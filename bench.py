@@ -68,7 +68,8 @@ def make_workload(name):
     return {'c1': W.c1, 'c2': W.c2, 'c3': W.c3, 'c5': W.c5, 'c3_small': W.c3_small}[name](0)
 
 
-def workload_config(wl, cache):
+def workload_config(wl, cache, world=1):
+    """The workload a line measures (identical in both arms)."""
     cfg = {'workload': f'{wl.name}: {wl.num_qubits}-qubit '
                        + ('JW molecular Hamiltonian, alpha x beta product subspace'
                           if wl.name in ('c2', 'c3', 'c3_small') else 'random Pauli sum, weight subspace'),
@@ -77,6 +78,7 @@ def workload_config(wl, cache):
            'cache_strategy': list(cache), 'vector_dtype': 'complex128',
            'l2': 'no flush: stored pairs read per step exceed the 126 MB L2'}
     cfg.update({k: v for k, v in wl.notes.items() if k in ('norb', 'nelec', 'na', 'nb')})
+    cfg['parallelism'] = f'replicas x{world}'
     return cfg
 
 
@@ -300,9 +302,12 @@ def run_reference(args):
             'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
             'ms_per_step': dt * 1e3, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'complex128 (f64 arithmetic)', 'data': 'synthetic',
-            'config': workload_config(wl, (1, 0)),
+            'config': workload_config(wl, tuple(int(v) for v in args.cache.split(',')),
+                                      args.gpus),
             'cpu_baseline': {'value': val, 'unit': UNIT, 'cores': cpu.nproc, 'kind': 'port',
-                             'sample': cpu_sample_desc(sample, n, cpu.num_terms)},
+                             'sample': cpu_sample_desc(sample, n, cpu.num_terms) +
+                                       ' (the same Hv as every cache strategy; the reference\'s '
+                                       'default (1, 0) algorithm)'},
             'e2e': {'value': val, 'unit': UNIT, 'h2d_bytes_per_step': 0,
                     'd2h_bytes_per_step': 0}}
     print(json.dumps(line), flush=True)
@@ -413,14 +418,13 @@ def run_ours(args):
             'dtype': ('complex128 (f64 arithmetic)' if prec == 0 else
                       'complex64 (f32 products, compensated sums, f64 partials)'),
             'data': 'synthetic (seeded generator)',
-            'config': {**workload_config(wl, cache), 'parallelism': f'replicas x{world}',
-                       'merged_terms': m_terms, 'x_groups': j_groups, 'stored_pairs': nnz,
-                       'lanes_per_row': {'fp64': op.get_lanes(0), 'fp32': op.get_lanes(1)},
-                       'layout': {'fp64': layout,
-                                  'fp32': op.get_layout(1) if cache == (1, 2) else 'csr'},
-                       'kernels_per_matvec': per_step, 'precision': args.precision,
-                       'autotune': tuned,
-                       'setup_s': setup_s},
+            'config': workload_config(wl, cache, world),
+            'schedule': {'merged_terms': m_terms, 'x_groups': j_groups, 'stored_pairs': nnz,
+                         'lanes_per_row': {'fp64': op.get_lanes(0), 'fp32': op.get_lanes(1)},
+                         'layout': {'fp64': layout,
+                                    'fp32': op.get_layout(1) if cache == (1, 2) else 'csr'},
+                         'kernels_per_matvec': per_step, 'precision': args.precision,
+                         'autotune': tuned, 'setup_s': setup_s},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                          'frac': achieved / peak, 'traffic': traffic,
                          'traffic_source': traffic_note,
