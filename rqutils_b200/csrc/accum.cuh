@@ -126,7 +126,7 @@ struct CAcc {
 };
 
 // One lane's share of a CSR row: pairs i0, i0 + LPR, ... below e.  Four pairs per step with
-// independent index -> amplitude gathers in flight, then the remainder as one predicated step.
+// independent index -> amplitude gathers in flight, then the remainder.
 // CG: read v through L2 (v written earlier in the same launch by other blocks).
 template <typename R, int NCV, int NCA, int LPR, bool CG = false>
 __device__ __forceinline__ void csr_row_dot(const uint32_t* __restrict__ cols,
@@ -146,22 +146,29 @@ __device__ __forceinline__ void csr_row_dot(const uint32_t* __restrict__ cols,
     }
     acc.add4(a, x);
   }
-  // The remainder (fewer than four pairs) as one predicated step, so its gathers are in flight
-  // together too (short rows, such as the two-half tails, are mostly remainder).  Absent pairs
-  // add exact zeros.
-  if (i < e) {
-    uint32_t c[4];
+  // The remainder (fewer than four pairs): for FP32 rows shared by at most four lanes (short
+  // rows, such as the two-half tails at 48 qubits) one predicated step, so its gathers are in
+  // flight together, absent pairs adding exact zeros; otherwise one pair at a time (measured
+  // faster there: FP64 tails, and FP32 rows spread over 8-16 lanes).
+  if constexpr (sizeof(R) == 4 && LPR <= 4) {
+    if (i < e) {
+      uint32_t c[4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) c[u] = (i + u * LPR < e) ? __ldg(cols + i + u * LPR) : 0u;
-    Cx<R> a[4], x[4];
+      for (int u = 0; u < 4; ++u) c[u] = (i + u * LPR < e) ? __ldg(cols + i + u * LPR) : 0u;
+      Cx<R> a[4], x[4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const bool ok = i + u * LPR < e;
-      a[u] = ok ? ld_elem<R, NCA>(vals, i + u * LPR) : cx_make<R>(R(0), R(0));
-      x[u] = ok ? (CG ? ld_elem_cg<R, NCV>(v, c[u]) : ld_elem<R, NCV>(v, c[u]))
-                : cx_make<R>(R(0), R(0));
+      for (int u = 0; u < 4; ++u) {
+        const bool ok = i + u * LPR < e;
+        a[u] = ok ? ld_elem<R, NCA>(vals, i + u * LPR) : cx_make<R>(R(0), R(0));
+        x[u] = ok ? (CG ? ld_elem_cg<R, NCV>(v, c[u]) : ld_elem<R, NCV>(v, c[u]))
+                  : cx_make<R>(R(0), R(0));
+      }
+      acc.add4(a, x);
     }
-    acc.add4(a, x);
+  } else {
+    for (; i < e; i += LPR)
+      acc.add(ld_elem<R, NCA>(vals, i),
+              CG ? ld_elem_cg<R, NCV>(v, __ldg(cols + i)) : ld_elem<R, NCV>(v, __ldg(cols + i)));
   }
 }
 

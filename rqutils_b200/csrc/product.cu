@@ -286,20 +286,11 @@ k_slab(int64_t A, int64_t B, int64_t total_k, int64_t a_tiles, const int64_t* __
       acc.add4(m + 4, xv + 4);
       vp += 8 * 32 * NCA;
     }
-    // remainder (fewer than eight entries): one predicated step, all gathers in flight
-    if (k < k1) {
-      uint32_t si[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) si[u] = (k + u < k1) ? __ldg(src + k + u) : 0u;
-      Cx<R> m[8], xv[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const bool ok = k + u < k1;
-        m[u] = ok ? ld_elem<R, NCA>(vp, 32 * u) : cx_make<R>(R(0), R(0));
-        xv[u] = ok ? ld_elem<R, NCV>(x, int64_t(si[u]) + b) : cx_make<R>(R(0), R(0));
-      }
-      acc.add4(m, xv);
-      acc.add4(m + 4, xv + 4);
+    // remainder: one entry at a time (a predicated eight-entry step measured 5-11 % slower
+    // for FP64 at 32 and 48 qubits)
+    for (; k < k1; ++k) {
+      acc.add(ld_elem<R, NCA>(vp, 0), ld_elem<R, NCV>(x, int64_t(__ldg(src + k)) + b));
+      vp += 32 * NCA;
     }
     if constexpr (FINAL) st_elem<R, NCV>(out, a * B + b, cx_make<R>(acc.re.value(), acc.im.value()));
     else acc.store_partial(out_part, a * B + b);
