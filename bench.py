@@ -326,10 +326,14 @@ def run_ours(args):
     ham = rq.PauliSumXZ.from_xz(wl.x, wl.z, wl.coeffs, wl.num_qubits, force_real=True,
                                 padded=True)
     space = rq.Subspace.from_u64(wl.states, wl.num_qubits)
+    torch.cuda.synchronize()
+    from rqutils_b200 import _lib
+    used0 = _lib.memory_stats()[1]
     t_setup0 = time.perf_counter()
     op = rq.SQDOperator(ham, space, cache_strategy=cache)
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t_setup0
+    used_op = _lib.memory_stats()[1] - used0
     if args.lanes:
         for prec in (0, 1):
             op.set_layout(prec, args.layout)
@@ -339,6 +343,8 @@ def run_ours(args):
                  'note': 'fixed by --layout/--lanes/--chunk'}
     else:
         tuned = op.autotune()
+    torch.cuda.synchronize()
+    used_tuned = _lib.memory_stats()[1] - used0
     n_rows = space.states_size
     m_terms = ham.num_terms
     j_groups = ham.num_groups
@@ -424,7 +430,12 @@ def run_ours(args):
                          'layout': {'fp64': layout,
                                     'fp32': op.get_layout(1) if cache == (1, 2) else 'csr'},
                          'kernels_per_matvec': per_step, 'precision': args.precision,
-                         'autotune': tuned, 'setup_s': setup_s},
+                         'autotune': tuned, 'setup_s': setup_s,
+                         'device_memory_bytes': {
+                             'operator': used_op, 'with_layouts': used_tuned,
+                             'note': 'library pool bytes in use for this cache strategy: the '
+                                     'operator as built, then with the matvec layouts the '
+                                     'schedule selected (FP32 copies, product slabs)'}},
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                          'frac': achieved / peak, 'traffic': traffic,
                          'traffic_source': traffic_note,
