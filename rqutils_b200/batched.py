@@ -108,7 +108,11 @@ def solve_instances(instances, budget_bytes=48 << 30, alone_pairs=int(1.5e9), to
                                    use_graph=use_graph, vspace=(op.size, dtype))
             eig[i], nit[i] = e, it
             del op
-            _lib.trim_memory()
+            # The library pool keeps the freed memory for the next wave's tables; return it to
+            # the driver only when little is left for other allocators (torch's vectors).
+            free, _ = torch.cuda.mem_get_info()
+            if free < (8 << 30):
+                _lib.trim_memory()
             continue
         need = op.nnz * 16 + op.size * 7 * 16
         if wave and wave_bytes + need > budget_bytes:
