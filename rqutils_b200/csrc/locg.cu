@@ -762,14 +762,16 @@ __global__ void k_convert(const RI* in, RO* out, int64_t n) {
 // The fast implicit iteration (5 fused passes + 1 cached CSR matvec) as ONE cooperative launch
 // that loops until the convergence step sets `done`.  On small operators the graph form is
 // bound by its ~6 dependent launches per iteration, each a few microseconds of launch and
-// drain; here the phases are separated by a grid barrier instead.  The last block to reach a
+// drain; here the iteration is four phases separated by grid barriers: the first projection
+// round, the second round fused with the matvec and the Gram dots (persist_gram_matvec), the
+// update and the convergence pass.  The last block to reach a
 // barrier sums the dot partials of all blocks (fixed order) before it releases the others;
 // every block then runs the scalar step on its own shared-memory copy of the solver state from
 // the same sums, so all blocks hold bit-identical coefficients without a second barrier;
 // block 0 writes the history rows and, at the end, the state back.
 // Vectors written within the launch are read through L2 (ld.global.cg).
 struct PersistArgs {
-  LCArgs<6, 10, 5> ps[5];      // body_fast's passes in order (the matvec follows ps[1])
+  LCArgs<6, 10, 5> ps[5];      // body_fast's passes in order (ps[1] folded into the matvec)
   const int64_t* row_ptr;      // cached CSR operator
   const uint32_t* cols;
   const void* vals;            // FP64 or FP32 elements, as the vectors
@@ -849,48 +851,15 @@ __device__ __forceinline__ bool persist_sync(const PersistArgs& pa, unsigned& ge
   }
 }
 
-// cpart (CLU only): the kernel's shared [2][20] partials, alternating per dot pass; every block
-// sums the blocks' partials through distributed shared memory in rank order.
-template <typename R, int NC, typename S, bool CLU>
-__device__ __forceinline__ bool persist_pass(const LCArgs<6, 10, 5>& a, LocgDev& sd,
-                                             const PersistArgs& pa, unsigned& gen,
-                                             double* cpart, int& buf) {
-  constexpr int NS = S::NS, NO = S::NO, ND = S::ND;
-  constexpr int NOA = NO > 0 ? NO : 1, NDA = ND > 0 ? ND : 1;
-  double acc[NDA][2];
-#pragma unroll
-  for (int d = 0; d < NDA; ++d) acc[d][0] = acc[d][1] = 0.0;
-  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-  constexpr int64_t EB = int64_t(sizeof(R)) * NC;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < a.n; i += stride) {
-    double2 sv[NS];
-#pragma unroll
-    for (int k = 0; k < NS; ++k) {
-      const Cx<R> v = ld_elem_cg<R, NC>(static_cast<const R*>(a.src[k]), i);
-      sv[k] = make_double2(double(v.re), double(v.im));
-    }
-    if (i + stride < a.n) {
-#pragma unroll
-      for (int k = 0; k < NS; ++k)
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(static_cast<const char*>(a.src[k]) +
-                                                       (i + stride) * EB));
-    }
-    double2 ov[NOA];
-#pragma unroll
-    for (int q = 0; q < NO; ++q) {
-      double2 t = make_double2(0.0, 0.0);
-#pragma unroll
-      for (int k = 0; k < NS; ++k)
-        t = cadd(t, cmul(make_double2(sd.coef[q][k][0], sd.coef[q][k][1]), sv[k]));
-      if constexpr (NC == 1) t.y = 0.0;
-      ov[q] = t;
-    }
-    DotLoop<S, 0, ND>::run(acc, sv, ov);
-#pragma unroll
-    for (int q = 0; q < NO; ++q)
-      if (a.out[q] != nullptr)
-        st_elem<R, NC>(static_cast<R*>(a.out[q]), i, cx_make<R>(R(ov[q].x), R(ov[q].y)));
-  }
+// End of a phase: the block's dot partials (acc: ND complex sums), then the barrier, after
+// which every block holds the sums in sd.red.  cpart (CLU only): the kernel's shared [2][20]
+// partials, alternating per dot phase; every block sums the blocks' partials through
+// distributed shared memory in rank order.
+template <int ND, bool CLU>
+__device__ __forceinline__ bool persist_finish(double (*acc)[2], LocgDev& sd,
+                                               const PersistArgs& pa, unsigned& gen,
+                                               double* cpart, int& buf) {
+  constexpr int NDA = ND > 0 ? ND : 1;
   double* part = pa.partials;
   if constexpr (ND > 0) {
     __shared__ double sred[NDA * 2][LC_THREADS / 32];
@@ -925,47 +894,291 @@ __device__ __forceinline__ bool persist_pass(const LCArgs<6, 10, 5>& a, LocgDev&
       buf ^= 1;
       __syncthreads();
     }
+    return true;
   } else if constexpr (ND > 0) {
-    if (!persist_barrier(pa.bar, gen, part, 2 * ND, pa.red, &sd)) return false;
+    return persist_barrier(pa.bar, gen, part, 2 * ND, pa.red, &sd);
   } else {
-    if (!persist_barrier(pa.bar, gen)) return false;
+    return persist_barrier(pa.bar, gen);
   }
+}
+
+// 16 bytes of a vector: VW = 16 / element bytes elements (2 for complex64, 1 for complex128).
+template <typename R, int NC>
+struct Chunk16 {
+  static constexpr int VW = 16 / static_cast<int>(sizeof(R) * NC);
+  R v[VW * NC];
+  __device__ __forceinline__ double2 elem(int e) const {
+    if constexpr (NC == 2) return make_double2(double(v[2 * e]), double(v[2 * e + 1]));
+    else return make_double2(double(v[e]), 0.0);
+  }
+  __device__ __forceinline__ void set(int e, double2 t) {
+    if constexpr (NC == 2) {
+      v[2 * e] = R(t.x);
+      v[2 * e + 1] = R(t.y);
+    } else {
+      v[e] = R(t.x);
+    }
+  }
+};
+static_assert(sizeof(Chunk16<float, 2>) == 16 && sizeof(Chunk16<double, 1>) == 16, "16 bytes");
+
+template <typename R, int NC>
+__device__ __forceinline__ Chunk16<R, NC> ld_chunk_cg(const R* p, int64_t j) {
+  const double2 raw = __ldcg(reinterpret_cast<const double2*>(p) + j);
+  Chunk16<R, NC> c;
+  memcpy(&c, &raw, 16);
+  return c;
+}
+
+template <typename R, int NC>
+__device__ __forceinline__ void st_chunk(R* p, int64_t j, const Chunk16<R, NC>& c) {
+  double2 raw;
+  memcpy(&raw, &c, 16);
+  reinterpret_cast<double2*>(p)[j] = raw;
+}
+
+// One elementwise pass: every element's NO outputs as combinations of its NS sources with the
+// coefficients in sd.coef, the ND dots, then the phase end and the post step.  Each thread
+// step moves 16 bytes of every vector (two complex64 elements, or one complex128), which puts
+// twice the bytes in flight per load as one complex64 element at a time; the vectors are
+// 16-byte aligned (the host checks), an odd last element is done on its own.
+template <typename R, int NC, typename S, bool CLU>
+__device__ __forceinline__ bool persist_pass(const LCArgs<6, 10, 5>& a, LocgDev& sd,
+                                             const PersistArgs& pa, unsigned& gen,
+                                             double* cpart, int& buf) {
+  constexpr int NS = S::NS, NO = S::NO, ND = S::ND;
+  constexpr int NOA = NO > 0 ? NO : 1, NDA = ND > 0 ? ND : 1;
+  constexpr int VW = Chunk16<R, NC>::VW;
+  double acc[NDA][2];
+#pragma unroll
+  for (int d = 0; d < NDA; ++d) acc[d][0] = acc[d][1] = 0.0;
+  auto combine = [&](const double2* sv, double2* ov) {
+#pragma unroll
+    for (int q = 0; q < NO; ++q) {
+      double2 t = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < NS; ++k)
+        t = cadd(t, cmul(make_double2(sd.coef[q][k][0], sd.coef[q][k][1]), sv[k]));
+      if constexpr (NC == 1) t.y = 0.0;
+      ov[q] = t;
+    }
+    DotLoop<S, 0, ND>::run(acc, sv, ov);
+  };
+  const int64_t tid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  const int64_t nvec = a.n / VW;
+  for (int64_t j = tid; j < nvec; j += stride) {
+    Chunk16<R, NC> raw[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) raw[k] = ld_chunk_cg<R, NC>(static_cast<const R*>(a.src[k]), j);
+    if (j + stride < nvec) {
+#pragma unroll
+      for (int k = 0; k < NS; ++k)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(static_cast<const char*>(a.src[k]) +
+                                                       (j + stride) * 16));
+    }
+    Chunk16<R, NC> res[NOA];
+#pragma unroll
+    for (int e = 0; e < VW; ++e) {
+      double2 sv[NS], ov[NOA];
+#pragma unroll
+      for (int k = 0; k < NS; ++k) sv[k] = raw[k].elem(e);
+      combine(sv, ov);
+#pragma unroll
+      for (int q = 0; q < NO; ++q) res[q].set(e, ov[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < NO; ++q)
+      if (a.out[q] != nullptr) st_chunk<R, NC>(static_cast<R*>(a.out[q]), j, res[q]);
+  }
+  if constexpr (VW > 1) {
+    for (int64_t i = nvec * VW + tid; i < a.n; i += stride) {
+      double2 sv[NS], ov[NOA];
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        const Cx<R> v = ld_elem_cg<R, NC>(static_cast<const R*>(a.src[k]), i);
+        sv[k] = make_double2(double(v.re), double(v.im));
+      }
+      combine(sv, ov);
+#pragma unroll
+      for (int q = 0; q < NO; ++q)
+        if (a.out[q] != nullptr)
+          st_elem<R, NC>(static_cast<R*>(a.out[q]), i, cx_make<R>(R(ov[q].x), R(ov[q].y)));
+    }
+  }
+  if (!persist_finish<ND, CLU>(acc, sd, pa, gen, cpart, buf)) return false;
   if (threadIdx.x == 0 && a.post != P_NONE) run_post(&sd, a.post, a.nsrc, 0, 0);
   __syncthreads();
   return true;
 }
 
-template <typename R, int NCV, int NCA, int LPR>
-__device__ __forceinline__ void persist_matvec(const PersistArgs& pa) {
-  constexpr int RPW = 32 / LPR;
-  const int lane = threadIdx.x & 31;
-  const int sub = lane % LPR, slot = lane / LPR;
-  const R* vals = static_cast<const R*>(pa.vals);
-  const R* v = static_cast<const R*>(pa.mv_in);
-  R* out = static_cast<R*>(pa.mv_out);
-  const int64_t w0 = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
-  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
-  for (int64_t rb = w0 * RPW; rb < pa.n; rb += nw * RPW) {
-    const int64_t row = rb + slot;
-    CAcc<R, NCV, NCA> acc;
-    if (row < pa.n) {
-      const int64_t b = __ldg(pa.row_ptr + row), e = __ldg(pa.row_ptr + row + 1);
-      csr_row_dot<R, NCV, NCA, LPR, true>(pa.cols, vals, v, b + sub, e, acc);
-    }
-    acc.merge(LPR);
-    if (sub == 0 && row < pa.n)
-      st_elem<R, NCV>(out, row, cx_make<R>(acc.re.value(), acc.im.value()));
-  }
-}
-
 using PShape0 = PassShape<3, 1, 100, 100, 1, 100, 2, 100>;
-using PShape1 = PassShape<3, 1>;
 using PShape2 = PassShape<6, 0, 0, 3, 1, 4, 2, 5, 1, 3, 2, 3, 2, 4, 2, 2, 1, 2>;
 using PShape3 = PassShape<6, 4, 100, 100, 101, 101>;
 using PShape4 = PassShape<4, 5, 104, 104, 102, 102, 100, 104, 101, 104>;
 
+// The second projection round of p, the matvec and the Gram pass of the fast iteration
+// (body_fast's passes 2 and 3 and its matvec) as ONE phase.  The second round forms
+// p = c0 p0 + c1 x + c2 y from the first round's p0 with the coefficients c of the first
+// round's post step; since A p = c0 A p0 + c1 A x + c2 A y and A x, A y are carried, the phase
+// gathers p0 (complete since the last barrier) for A p0, stores A p0 where A p would go, forms
+// p and A p of its own rows in registers for the Gram dots, and once the Rayleigh-Ritz step has
+// set the update pass's coefficients over (x, y, p, A x, A y, A p), folds c into them so that
+// the update pass reads p0 and A p0 instead.  Relative to c0, c1 and c2 are the second round's
+// corrections, of the order of the first round's rounding error, so the carried A x, A y enter
+// with that weight.  This saves two grid barriers and four vector streams per iteration.
+// Rows: LPR lanes per row (the row's elementwise operands are loaded by its first lane before
+// the row's pair loads are issued); with LPR = 1 (rows of about one stored pair, such as
+// near-diagonal operators) a thread takes two or four consecutive rows per step.
 template <typename R, int NC, int NCA, int LPR, bool CLU>
-__global__ void __launch_bounds__(LC_THREADS, 3) k_locg_persist(PersistArgs pa) {
+__device__ __forceinline__ bool persist_gram_matvec(const PersistArgs& pa, LocgDev& sd,
+                                                    unsigned& gen, double* cpart, int& buf) {
+  using S = PShape2;   // sources x, y, p, A x, A y, A p; eight dots
+  constexpr int ND = S::ND;
+  const LCArgs<6, 10, 5>& g = pa.ps[2];
+  const R* xs = static_cast<const R*>(g.src[0]);
+  const R* ys = static_cast<const R*>(g.src[1]);
+  const R* p0 = static_cast<const R*>(pa.mv_in);
+  const R* axs = static_cast<const R*>(g.src[3]);
+  const R* ays = static_cast<const R*>(g.src[4]);
+  const R* vals = static_cast<const R*>(pa.vals);
+  R* ap0 = static_cast<R*>(pa.mv_out);
+  const double2 c0 = make_double2(sd.coef[0][0][0], sd.coef[0][0][1]);
+  const double2 c1 = make_double2(sd.coef[0][1][0], sd.coef[0][1][1]);
+  const double2 c2 = make_double2(sd.coef[0][2][0], sd.coef[0][2][1]);
+  double acc[ND][2];
+#pragma unroll
+  for (int d = 0; d < ND; ++d) acc[d][0] = acc[d][1] = 0.0;
+  auto d2 = [](Cx<R> v) { return make_double2(double(v.re), double(v.im)); };
+  // A p0 of the row is m; x..ay its elementwise operands.
+  auto finish = [&](int64_t row, const CAcc<R, NC, NCA>& m, Cx<R> x, Cx<R> y, Cx<R> p,
+                    Cx<R> ax, Cx<R> ay) {
+    const Cx<R> a0 = cx_make<R>(m.re.value(), m.im.value());
+    st_elem<R, NC>(ap0, row, a0);
+    double2 sv[6];
+    sv[0] = d2(x);
+    sv[1] = d2(y);
+    sv[3] = d2(ax);
+    sv[4] = d2(ay);
+    sv[2] = cadd(cmul(c0, d2(p)), cadd(cmul(c1, sv[0]), cmul(c2, sv[1])));
+    sv[5] = cadd(cmul(c0, d2(a0)), cadd(cmul(c1, sv[3]), cmul(c2, sv[4])));
+    if constexpr (NC == 1) sv[2].y = sv[5].y = 0.0;
+    DotLoop<S, 0, ND>::run(acc, sv, sv);
+  };
+  const Cx<R> zero = cx_make<R>(R(0), R(0));
+  if constexpr (LPR == 1) {
+    // ROWS consecutive rows per thread step (one 16-byte chunk of every vector for complex64,
+    // two for complex128): their pair chains are in flight together and their elementwise
+    // operands arrive as chunk loads.
+    constexpr int VW = Chunk16<R, NC>::VW;
+    constexpr int ROWS = VW > 2 ? VW : 2;
+    constexpr int NCH = ROWS / VW;
+    const int64_t tid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    const int64_t T = int64_t(gridDim.x) * blockDim.x;
+    const int64_t nsteps = pa.n / ROWS;
+    for (int64_t j = tid; j < nsteps; j += T) {
+      const int64_t row0 = j * ROWS;
+      Chunk16<R, NC> cx[NCH], cy[NCH], cp[NCH], cax[NCH], cay[NCH];
+#pragma unroll
+      for (int h = 0; h < NCH; ++h) {
+        cx[h] = ld_chunk_cg<R, NC>(xs, j * NCH + h);
+        cy[h] = ld_chunk_cg<R, NC>(ys, j * NCH + h);
+        cp[h] = ld_chunk_cg<R, NC>(p0, j * NCH + h);
+        cax[h] = ld_chunk_cg<R, NC>(axs, j * NCH + h);
+        cay[h] = ld_chunk_cg<R, NC>(ays, j * NCH + h);
+      }
+      int64_t bnd[ROWS + 1];
+#pragma unroll
+      for (int u = 0; u <= ROWS; ++u) bnd[u] = __ldg(pa.row_ptr + row0 + u);
+      uint32_t c[ROWS];
+#pragma unroll
+      for (int u = 0; u < ROWS; ++u) c[u] = bnd[u] < bnd[u + 1] ? __ldg(pa.cols + bnd[u]) : 0u;
+      CAcc<R, NC, NCA> m[ROWS];
+#pragma unroll
+      for (int u = 0; u < ROWS; ++u)
+        if (bnd[u] < bnd[u + 1])
+          m[u].add(ld_elem<R, NCA>(vals, bnd[u]), ld_elem_cg<R, NC>(p0, c[u]));
+#pragma unroll
+      for (int u = 0; u < ROWS; ++u)
+        if (bnd[u] + 1 < bnd[u + 1])
+          csr_row_dot<R, NC, NCA, 1, true>(pa.cols, vals, p0, bnd[u] + 1, bnd[u + 1], m[u]);
+      Chunk16<R, NC> ca[NCH];
+#pragma unroll
+      for (int u = 0; u < ROWS; ++u) {
+        const Cx<R> a0 = cx_make<R>(m[u].re.value(), m[u].im.value());
+        ca[u / VW].set(u % VW, d2(a0));
+        double2 sv[6];
+        sv[0] = cx[u / VW].elem(u % VW);
+        sv[1] = cy[u / VW].elem(u % VW);
+        sv[3] = cax[u / VW].elem(u % VW);
+        sv[4] = cay[u / VW].elem(u % VW);
+        sv[2] = cadd(cmul(c0, cp[u / VW].elem(u % VW)), cadd(cmul(c1, sv[0]), cmul(c2, sv[1])));
+        sv[5] = cadd(cmul(c0, d2(a0)), cadd(cmul(c1, sv[3]), cmul(c2, sv[4])));
+        if constexpr (NC == 1) sv[2].y = sv[5].y = 0.0;
+        DotLoop<S, 0, ND>::run(acc, sv, sv);
+      }
+#pragma unroll
+      for (int h = 0; h < NCH; ++h) st_chunk<R, NC>(ap0, j * NCH + h, ca[h]);
+    }
+    for (int64_t row = nsteps * ROWS + tid; row < pa.n; row += T) {
+      CAcc<R, NC, NCA> m;
+      csr_row_dot<R, NC, NCA, 1, true>(pa.cols, vals, p0, __ldg(pa.row_ptr + row),
+                                       __ldg(pa.row_ptr + row + 1), m);
+      finish(row, m, ld_elem_cg<R, NC>(xs, row), ld_elem_cg<R, NC>(ys, row),
+             ld_elem_cg<R, NC>(p0, row), ld_elem_cg<R, NC>(axs, row), ld_elem_cg<R, NC>(ays, row));
+    }
+  } else {
+    constexpr int RPW = 32 / LPR;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane % LPR, slot = lane / LPR;
+    const int64_t w0 = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5;
+    const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t rb = w0 * RPW; rb < pa.n; rb += nw * RPW) {
+      const int64_t row = rb + slot;
+      const bool live = row < pa.n, lead = live && sub == 0;
+      const Cx<R> ex = lead ? ld_elem_cg<R, NC>(xs, row) : zero;
+      const Cx<R> ey = lead ? ld_elem_cg<R, NC>(ys, row) : zero;
+      const Cx<R> ep = lead ? ld_elem_cg<R, NC>(p0, row) : zero;
+      const Cx<R> eax = lead ? ld_elem_cg<R, NC>(axs, row) : zero;
+      const Cx<R> eay = lead ? ld_elem_cg<R, NC>(ays, row) : zero;
+      CAcc<R, NC, NCA> m;
+      if (live) {
+        const int64_t b = __ldg(pa.row_ptr + row), e = __ldg(pa.row_ptr + row + 1);
+        csr_row_dot<R, NC, NCA, LPR, true>(pa.cols, vals, p0, b + sub, e, m);
+      }
+      m.merge(LPR);
+      if (lead) finish(row, m, ex, ey, ep, eax, eay);
+    }
+  }
+  if (!persist_finish<ND, CLU>(acc, sd, pa, gen, cpart, buf)) return false;
+  if (threadIdx.x == 0) {
+    run_post(&sd, g.post, g.nsrc, 0, 0);
+    if (!sd.done) {
+      // update pass: x, y over sources (x, y, p) = columns 0-2, A x, A y over columns 3-5
+      for (int o = 0; o < 4; ++o) {
+        const int q0 = o < 2 ? 0 : 3;
+        const double2 k = make_double2(sd.coef[o][q0 + 2][0], sd.coef[o][q0 + 2][1]);
+        const double2 a = cadd(make_double2(sd.coef[o][q0][0], sd.coef[o][q0][1]), cmul(k, c1));
+        const double2 b = cadd(make_double2(sd.coef[o][q0 + 1][0], sd.coef[o][q0 + 1][1]),
+                               cmul(k, c2));
+        const double2 f = cmul(k, c0);
+        sd.coef[o][q0][0] = a.x;
+        sd.coef[o][q0][1] = a.y;
+        sd.coef[o][q0 + 1][0] = b.x;
+        sd.coef[o][q0 + 1][1] = b.y;
+        sd.coef[o][q0 + 2][0] = f.x;
+        sd.coef[o][q0 + 2][1] = f.y;
+      }
+    }
+  }
+  __syncthreads();
+  return true;
+}
+
+// Two blocks per SM: the FP32 passes' 16-byte steps and the Gram phase's eight FP64 dot sums
+// need up to 128 registers a thread (with three blocks per SM, 85, they spilled 0.5-1 KB).
+template <typename R, int NC, int NCA, int LPR, bool CLU>
+__global__ void __launch_bounds__(LC_THREADS, 2) k_locg_persist(PersistArgs pa) {
   __shared__ LocgDev sd;
   __shared__ double cpart[2 * 20];
   {
@@ -981,10 +1194,8 @@ __global__ void __launch_bounds__(LC_THREADS, 3) k_locg_persist(PersistArgs pa) 
   int buf = 0;
   for (int it = 0; it < pa.max_iter && !sd.done; ++it) {
     if (!persist_pass<R, NC, PShape0, CLU>(pa.ps[0], sd, pa, gen, cpart, buf)) return;
-    if (!persist_pass<R, NC, PShape1, CLU>(pa.ps[1], sd, pa, gen, cpart, buf)) return;
-    persist_matvec<R, NC, NCA, LPR>(pa);
-    if (!persist_sync<CLU>(pa, gen)) return;
-    if (!persist_pass<R, NC, PShape2, CLU>(pa.ps[2], sd, pa, gen, cpart, buf)) return;
+    if (!persist_gram_matvec<R, NC, NCA, LPR, CLU>(pa, sd, gen, cpart, buf)) return;
+    if (sd.done) break;   // the Rayleigh-Ritz step found nothing left to improve
     if (!persist_pass<R, NC, PShape3, CLU>(pa.ps[3], sd, pa, gen, cpart, buf)) return;
     if (!persist_pass<R, NC, PShape4, CLU>(pa.ps[4], sd, pa, gen, cpart, buf)) return;
   }
@@ -1275,7 +1486,7 @@ class Locg {
             bool fast = false) {
     read_host();
     if (maxiter <= 0 || host_->done) return;
-    if (fast && use_graph && orth.empty() && persist_op_ != nullptr) {
+    if (fast && use_graph && orth.empty() && persist_op_ != nullptr && persist_aligned()) {
       loop_persistent(maxiter);
       return;
     }
@@ -1402,6 +1613,13 @@ class Locg {
   // The fast iteration may run as one persistent launch (k_locg_persist) when the matvec is
   // this cached operator's CSR kernel; nullptr keeps the graph form.
   void set_persistent_op(sqd_op_s* op) { persist_op_ = op; }
+  // The persistent passes move 16 bytes of every vector per thread step.
+  bool persist_aligned() const {
+    const R* vecs[] = {x_.ptr, y_.ptr, r_.ptr, p_.ptr, ax_.ptr, ay_.ptr, ap_.ptr};
+    for (const R* v : vecs)
+      if (reinterpret_cast<uintptr_t>(v) % 16 != 0) return false;
+    return true;
+  }
 
  private:
   // Small vectors (at most kClusterMax blocks' worth): the grid is one thread-block cluster,
@@ -1484,7 +1702,8 @@ class Locg {
     // Lanes per row from the mean row length, not the standalone matvec's tuned value: inside
     // the persistent launch the grid is small and a row's lanes should not exceed its pairs.
     const double avg = n_ > 0 ? static_cast<double>(op->nnz) / static_cast<double>(n_) : 0.0;
-    const int lpr = avg >= 96 ? 32 : avg >= 40 ? 16 : avg >= 16 ? 8 : avg >= 6 ? 4 : 2;
+    const int lpr = avg >= 96 ? 32 : avg >= 40 ? 16 : avg >= 16 ? 8 : avg >= 6 ? 4
+                  : avg >= 2 ? 2 : 1;
     dispatch_lpr(lpr, [&](auto lpr_t) {
       constexpr int LPR = decltype(lpr_t)::value;
       if constexpr (NC == 2) {
@@ -2487,7 +2706,8 @@ extern "C" int sqd_batch_create(const sqd_op_t* ops, int n_ops, void* stream,
     SQD_CUDA(cudaMemcpyAsync(b->inst_tile0_d.ptr, b->inst_tile0.data(),
                              sizeof(int32_t) * (n_ops + 1), cudaMemcpyHostToDevice, st));
     const double avg = b->total_rows > 0 ? double(b->total_nnz) / double(b->total_rows) : 0.0;
-    const int lpr = avg >= 96 ? 32 : avg >= 40 ? 16 : avg >= 16 ? 8 : avg >= 6 ? 4 : 2;
+    const int lpr = avg >= 96 ? 32 : avg >= 40 ? 16 : avg >= 16 ? 8 : avg >= 6 ? 4
+                  : avg >= 2 ? 2 : 1;
     b->lanes[0] = b->lanes[1] = lpr;
     SQD_CUDA(cudaStreamSynchronize(st));
     *out = b.release();
