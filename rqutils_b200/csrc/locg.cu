@@ -762,16 +762,19 @@ __global__ void k_convert(const RI* in, RO* out, int64_t n) {
 // The fast implicit iteration (5 fused passes + 1 cached CSR matvec) as ONE cooperative launch
 // that loops until the convergence step sets `done`.  On small operators the graph form is
 // bound by its ~6 dependent launches per iteration, each a few microseconds of launch and
-// drain; here the iteration is four phases separated by grid barriers: the first projection
-// round, the second round fused with the matvec and the Gram dots (persist_gram_matvec), the
-// update and the convergence pass.  The last block to reach a
+// drain; here the iteration is three phases separated by grid barriers: the first projection
+// round, the second round fused with the matvec and the Gram dots (persist_gram_matvec), and
+// the update with the residual and the convergence dots (PShapeU).  The last block to reach a
 // barrier sums the dot partials of all blocks (fixed order) before it releases the others;
 // every block then runs the scalar step on its own shared-memory copy of the solver state from
 // the same sums, so all blocks hold bit-identical coefficients without a second barrier;
 // block 0 writes the history rows and, at the end, the state back.
 // Vectors written within the launch are read through L2 (ld.global.cg).
 struct PersistArgs {
-  LCArgs<6, 10, 5> ps[5];      // body_fast's passes in order (ps[1] folded into the matvec)
+  // ps[0]: first projection round; ps[2]: the Gram dots' sources (x, y, p, A x, A y, A p);
+  // ps[3]: the update pass (PShapeU).  ps[1] and ps[4] are not used: the second projection
+  // round is folded into the Gram-matvec phase and the normalisation into the scales.
+  LCArgs<6, 10, 5> ps[5];
   const int64_t* row_ptr;      // cached CSR operator
   const uint32_t* cols;
   const void* vals;            // FP64 or FP32 elements, as the vectors
@@ -902,10 +905,14 @@ __device__ __forceinline__ bool persist_finish(double (*acc)[2], LocgDev& sd,
   }
 }
 
-// 16 bytes of a vector: VW = 16 / element bytes elements (2 for complex64, 1 for complex128).
+// A thread step's share of a vector: two elements (8 bytes for float, 16 for complex64 or
+// double), or one complex128 element (16 bytes).
 template <typename R, int NC>
-struct Chunk16 {
-  static constexpr int VW = 16 / static_cast<int>(sizeof(R) * NC);
+struct VChunk {
+  static constexpr int EB = static_cast<int>(sizeof(R)) * NC;   // bytes per element
+  static constexpr int VW = EB >= 16 ? 1 : 2;
+  static constexpr int BYTES = VW * EB;
+  using Raw = std::conditional_t<BYTES == 16, double2, unsigned long long>;
   R v[VW * NC];
   __device__ __forceinline__ double2 elem(int e) const {
     if constexpr (NC == 2) return make_double2(double(v[2 * e]), double(v[2 * e + 1]));
@@ -920,35 +927,39 @@ struct Chunk16 {
     }
   }
 };
-static_assert(sizeof(Chunk16<float, 2>) == 16 && sizeof(Chunk16<double, 1>) == 16, "16 bytes");
+static_assert(sizeof(VChunk<float, 2>) == 16 && sizeof(VChunk<float, 1>) == 8 &&
+              sizeof(VChunk<double, 1>) == 16 && sizeof(VChunk<double, 2>) == 16, "chunks");
 
 template <typename R, int NC>
-__device__ __forceinline__ Chunk16<R, NC> ld_chunk_cg(const R* p, int64_t j) {
-  const double2 raw = __ldcg(reinterpret_cast<const double2*>(p) + j);
-  Chunk16<R, NC> c;
-  memcpy(&c, &raw, 16);
+__device__ __forceinline__ VChunk<R, NC> ld_chunk_cg(const R* p, int64_t j) {
+  using Raw = typename VChunk<R, NC>::Raw;
+  const Raw raw = __ldcg(reinterpret_cast<const Raw*>(p) + j);
+  VChunk<R, NC> c;
+  memcpy(&c, &raw, sizeof(Raw));
   return c;
 }
 
 template <typename R, int NC>
-__device__ __forceinline__ void st_chunk(R* p, int64_t j, const Chunk16<R, NC>& c) {
-  double2 raw;
-  memcpy(&raw, &c, 16);
-  reinterpret_cast<double2*>(p)[j] = raw;
+__device__ __forceinline__ void st_chunk(R* p, int64_t j, const VChunk<R, NC>& c) {
+  using Raw = typename VChunk<R, NC>::Raw;
+  Raw raw;
+  memcpy(&raw, &c, sizeof(Raw));
+  reinterpret_cast<Raw*>(p)[j] = raw;
 }
 
-// One elementwise pass: every element's NO outputs as combinations of its NS sources with the
-// coefficients in sd.coef, the ND dots, then the phase end and the post step.  Each thread
-// step moves 16 bytes of every vector (two complex64 elements, or one complex128), which puts
-// twice the bytes in flight per load as one complex64 element at a time; the vectors are
-// 16-byte aligned (the host checks), an odd last element is done on its own.
+// One elementwise pass: every element's NO outputs as combinations of its NS sources (each
+// times its scale sc[k], see k_locg_persist) with the coefficients in sd.coef, the ND dots,
+// then the phase end and the post step.  Each thread step moves two elements of every vector
+// (one complex128; 16 bytes for complex64), which puts twice the bytes in flight per load as
+// one element at a time; the vectors are 16-byte aligned (the host checks), an odd last
+// element is done on its own.
 template <typename R, int NC, typename S, bool CLU>
 __device__ __forceinline__ bool persist_pass(const LCArgs<6, 10, 5>& a, LocgDev& sd,
                                              const PersistArgs& pa, unsigned& gen,
-                                             double* cpart, int& buf) {
+                                             double* cpart, int& buf, const double* sc) {
   constexpr int NS = S::NS, NO = S::NO, ND = S::ND;
   constexpr int NOA = NO > 0 ? NO : 1, NDA = ND > 0 ? ND : 1;
-  constexpr int VW = Chunk16<R, NC>::VW;
+  constexpr int VW = VChunk<R, NC>::VW;
   double acc[NDA][2];
 #pragma unroll
   for (int d = 0; d < NDA; ++d) acc[d][0] = acc[d][1] = 0.0;
@@ -968,21 +979,21 @@ __device__ __forceinline__ bool persist_pass(const LCArgs<6, 10, 5>& a, LocgDev&
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   const int64_t nvec = a.n / VW;
   for (int64_t j = tid; j < nvec; j += stride) {
-    Chunk16<R, NC> raw[NS];
+    VChunk<R, NC> raw[NS];
 #pragma unroll
     for (int k = 0; k < NS; ++k) raw[k] = ld_chunk_cg<R, NC>(static_cast<const R*>(a.src[k]), j);
     if (j + stride < nvec) {
 #pragma unroll
       for (int k = 0; k < NS; ++k)
         asm volatile("prefetch.global.L2 [%0];" ::"l"(static_cast<const char*>(a.src[k]) +
-                                                       (j + stride) * 16));
+                                                       (j + stride) * VChunk<R, NC>::BYTES));
     }
-    Chunk16<R, NC> res[NOA];
+    VChunk<R, NC> res[NOA];
 #pragma unroll
     for (int e = 0; e < VW; ++e) {
       double2 sv[NS], ov[NOA];
 #pragma unroll
-      for (int k = 0; k < NS; ++k) sv[k] = raw[k].elem(e);
+      for (int k = 0; k < NS; ++k) sv[k] = cscale(raw[k].elem(e), sc[k]);
       combine(sv, ov);
 #pragma unroll
       for (int q = 0; q < NO; ++q) res[q].set(e, ov[q]);
@@ -997,7 +1008,7 @@ __device__ __forceinline__ bool persist_pass(const LCArgs<6, 10, 5>& a, LocgDev&
 #pragma unroll
       for (int k = 0; k < NS; ++k) {
         const Cx<R> v = ld_elem_cg<R, NC>(static_cast<const R*>(a.src[k]), i);
-        sv[k] = make_double2(double(v.re), double(v.im));
+        sv[k] = cscale(make_double2(double(v.re), double(v.im)), sc[k]);
       }
       combine(sv, ov);
 #pragma unroll
@@ -1014,8 +1025,22 @@ __device__ __forceinline__ bool persist_pass(const LCArgs<6, 10, 5>& a, LocgDev&
 
 using PShape0 = PassShape<3, 1, 100, 100, 1, 100, 2, 100>;
 using PShape2 = PassShape<6, 0, 0, 3, 1, 4, 2, 5, 1, 3, 2, 3, 2, 4, 2, 2, 1, 2>;
-using PShape3 = PassShape<6, 4, 100, 100, 101, 101>;
-using PShape4 = PassShape<4, 5, 104, 104, 102, 102, 100, 104, 101, 104>;
+// The update pass of the persistent iteration: u, t, A u, A t and r' = A u - theta u from
+// (x, y, p0, A x, A y, A p0), unnormalised, with |u|^2, |t|^2, |r'|^2, |A u|^2, <u|r'>, <t|r'>.
+// body_fast normalises in a pass of its own (x, y, A x, A y read and written once more, r
+// written); here the norms become the scales the next passes apply as they load.
+using PShapeU = PassShape<6, 5, 100, 100, 101, 101, 104, 104, 102, 102, 100, 104, 101, 104>;
+
+// x[i] *= s, in place (the final normalisation of a persistent loop).
+template <typename R, int NC>
+struct PersistNorm {
+  R* p;
+  double s;
+  __device__ __forceinline__ void apply(int64_t i) const {
+    const Cx<R> v = ld_elem_cg<R, NC>(p, i);
+    st_elem<R, NC>(p, i, cx_make<R>(R(double(v.re) * s), R(double(v.im) * s)));
+  }
+};
 
 // The second projection round of p, the matvec and the Gram pass of the fast iteration
 // (body_fast's passes 2 and 3 and its matvec) as ONE phase.  The second round forms
@@ -1032,7 +1057,8 @@ using PShape4 = PassShape<4, 5, 104, 104, 102, 102, 100, 104, 101, 104>;
 // near-diagonal operators) a thread takes two or four consecutive rows per step.
 template <typename R, int NC, int NCA, int LPR, bool CLU>
 __device__ __forceinline__ bool persist_gram_matvec(const PersistArgs& pa, LocgDev& sd,
-                                                    unsigned& gen, double* cpart, int& buf) {
+                                                    unsigned& gen, double* cpart, int& buf,
+                                                    const double* vs) {
   using S = PShape2;   // sources x, y, p, A x, A y, A p; eight dots
   constexpr int ND = S::ND;
   const LCArgs<6, 10, 5>& g = pa.ps[2];
@@ -1046,6 +1072,7 @@ __device__ __forceinline__ bool persist_gram_matvec(const PersistArgs& pa, LocgD
   const double2 c0 = make_double2(sd.coef[0][0][0], sd.coef[0][0][1]);
   const double2 c1 = make_double2(sd.coef[0][1][0], sd.coef[0][1][1]);
   const double2 c2 = make_double2(sd.coef[0][2][0], sd.coef[0][2][1]);
+  const double sx = vs[0], sy = vs[1];   // stored x, A x and y, A y times these
   double acc[ND][2];
 #pragma unroll
   for (int d = 0; d < ND; ++d) acc[d][0] = acc[d][1] = 0.0;
@@ -1056,10 +1083,10 @@ __device__ __forceinline__ bool persist_gram_matvec(const PersistArgs& pa, LocgD
     const Cx<R> a0 = cx_make<R>(m.re.value(), m.im.value());
     st_elem<R, NC>(ap0, row, a0);
     double2 sv[6];
-    sv[0] = d2(x);
-    sv[1] = d2(y);
-    sv[3] = d2(ax);
-    sv[4] = d2(ay);
+    sv[0] = cscale(d2(x), sx);
+    sv[1] = cscale(d2(y), sy);
+    sv[3] = cscale(d2(ax), sx);
+    sv[4] = cscale(d2(ay), sy);
     sv[2] = cadd(cmul(c0, d2(p)), cadd(cmul(c1, sv[0]), cmul(c2, sv[1])));
     sv[5] = cadd(cmul(c0, d2(a0)), cadd(cmul(c1, sv[3]), cmul(c2, sv[4])));
     if constexpr (NC == 1) sv[2].y = sv[5].y = 0.0;
@@ -1070,7 +1097,7 @@ __device__ __forceinline__ bool persist_gram_matvec(const PersistArgs& pa, LocgD
     // ROWS consecutive rows per thread step (one 16-byte chunk of every vector for complex64,
     // two for complex128): their pair chains are in flight together and their elementwise
     // operands arrive as chunk loads.
-    constexpr int VW = Chunk16<R, NC>::VW;
+    constexpr int VW = VChunk<R, NC>::VW;
     constexpr int ROWS = VW > 2 ? VW : 2;
     constexpr int NCH = ROWS / VW;
     const int64_t tid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
@@ -1078,7 +1105,7 @@ __device__ __forceinline__ bool persist_gram_matvec(const PersistArgs& pa, LocgD
     const int64_t nsteps = pa.n / ROWS;
     for (int64_t j = tid; j < nsteps; j += T) {
       const int64_t row0 = j * ROWS;
-      Chunk16<R, NC> cx[NCH], cy[NCH], cp[NCH], cax[NCH], cay[NCH];
+      VChunk<R, NC> cx[NCH], cy[NCH], cp[NCH], cax[NCH], cay[NCH];
 #pragma unroll
       for (int h = 0; h < NCH; ++h) {
         cx[h] = ld_chunk_cg<R, NC>(xs, j * NCH + h);
@@ -1102,16 +1129,16 @@ __device__ __forceinline__ bool persist_gram_matvec(const PersistArgs& pa, LocgD
       for (int u = 0; u < ROWS; ++u)
         if (bnd[u] + 1 < bnd[u + 1])
           csr_row_dot<R, NC, NCA, 1, true>(pa.cols, vals, p0, bnd[u] + 1, bnd[u + 1], m[u]);
-      Chunk16<R, NC> ca[NCH];
+      VChunk<R, NC> ca[NCH];
 #pragma unroll
       for (int u = 0; u < ROWS; ++u) {
         const Cx<R> a0 = cx_make<R>(m[u].re.value(), m[u].im.value());
         ca[u / VW].set(u % VW, d2(a0));
         double2 sv[6];
-        sv[0] = cx[u / VW].elem(u % VW);
-        sv[1] = cy[u / VW].elem(u % VW);
-        sv[3] = cax[u / VW].elem(u % VW);
-        sv[4] = cay[u / VW].elem(u % VW);
+        sv[0] = cscale(cx[u / VW].elem(u % VW), sx);
+        sv[1] = cscale(cy[u / VW].elem(u % VW), sy);
+        sv[3] = cscale(cax[u / VW].elem(u % VW), sx);
+        sv[4] = cscale(cay[u / VW].elem(u % VW), sy);
         sv[2] = cadd(cmul(c0, cp[u / VW].elem(u % VW)), cadd(cmul(c1, sv[0]), cmul(c2, sv[1])));
         sv[5] = cadd(cmul(c0, d2(a0)), cadd(cmul(c1, sv[3]), cmul(c2, sv[4])));
         if constexpr (NC == 1) sv[2].y = sv[5].y = 0.0;
@@ -1169,6 +1196,11 @@ __device__ __forceinline__ bool persist_gram_matvec(const PersistArgs& pa, LocgD
         sd.coef[o][q0 + 2][0] = f.x;
         sd.coef[o][q0 + 2][1] = f.y;
       }
+      // fifth output of the update pass: r' = A u - theta u (the residual times |u|)
+      for (int q = 0; q < 6; ++q) {
+        sd.coef[4][q][0] = q < 3 ? -sd.theta * sd.coef[0][q][0] : sd.coef[2][q][0];
+        sd.coef[4][q][1] = q < 3 ? -sd.theta * sd.coef[0][q][1] : sd.coef[2][q][1];
+      }
     }
   }
   __syncthreads();
@@ -1187,17 +1219,69 @@ __global__ void __launch_bounds__(LC_THREADS, 2) k_locg_persist(PersistArgs pa) 
     for (int i = threadIdx.x; i < int(sizeof(LocgDev) / sizeof(long long)); i += blockDim.x)
       dst[i] = __ldcg(src + i);
   }
+  // vs: the stored x, A x, r times vs[0] and y, A y times vs[1] are the iteration's (normalised)
+  // vectors; sc0, scu: the per-source scales of the first projection and the update pass.
+  __shared__ double vs[2], sc0[3], scu[6];
+  if (threadIdx.x < 6) {
+    scu[threadIdx.x] = 1.0;
+    if (threadIdx.x < 3) sc0[threadIdx.x] = 1.0;
+    if (threadIdx.x < 2) vs[threadIdx.x] = 1.0;
+  }
   __syncthreads();
   if (blockIdx.x != 0 && threadIdx.x == 0) sd.hist = nullptr;   // block 0 records
   __syncthreads();
   unsigned gen = 0;
   int buf = 0;
   for (int it = 0; it < pa.max_iter && !sd.done; ++it) {
-    if (!persist_pass<R, NC, PShape0, CLU>(pa.ps[0], sd, pa, gen, cpart, buf)) return;
-    if (!persist_gram_matvec<R, NC, NCA, LPR, CLU>(pa, sd, gen, cpart, buf)) return;
+    if (!persist_pass<R, NC, PShape0, CLU>(pa.ps[0], sd, pa, gen, cpart, buf, sc0)) return;
+    if (!persist_gram_matvec<R, NC, NCA, LPR, CLU>(pa, sd, gen, cpart, buf, vs)) return;
     if (sd.done) break;   // the Rayleigh-Ritz step found nothing left to improve
-    if (!persist_pass<R, NC, PShape3, CLU>(pa.ps[3], sd, pa, gen, cpart, buf)) return;
-    if (!persist_pass<R, NC, PShape4, CLU>(pa.ps[4], sd, pa, gen, cpart, buf)) return;
+    if (!persist_pass<R, NC, PShapeU, CLU>(pa.ps[3], sd, pa, gen, cpart, buf, scu)) return;
+    if (threadIdx.x == 0) {
+      // red: |u|^2, |t|^2, |r'|^2, |A u|^2, <u|r'>, <t|r'> of the stored (unnormalised) update;
+      // the convergence step wants |r|^2, |A x|^2, <x|r>, <y|r> of x = u/|u|, y = t/|t|,
+      // r = r'/|u|.
+      const double cu = 1.0 / sqrt(sd.red[0][0]), ct = 1.0 / sqrt(sd.red[1][0]);
+      const double rr = cu * cu * sd.red[2][0], axax = cu * cu * sd.red[3][0];
+      const double xr0 = cu * cu * sd.red[4][0], xr1 = cu * cu * sd.red[4][1];
+      const double yr0 = cu * ct * sd.red[5][0], yr1 = cu * ct * sd.red[5][1];
+      sd.red[0][0] = rr;
+      sd.red[0][1] = 0.0;
+      sd.red[1][0] = axax;
+      sd.red[1][1] = 0.0;
+      sd.red[2][0] = xr0;
+      sd.red[2][1] = xr1;
+      sd.red[3][0] = yr0;
+      sd.red[3][1] = yr1;
+      run_post(&sd, P_CONV_PROJ, 4, 0, 0);
+      vs[0] = cu;
+      vs[1] = ct;
+      sc0[0] = cu;   // r
+      sc0[1] = cu;   // x
+      sc0[2] = ct;   // y
+      scu[0] = cu;   // x
+      scu[1] = ct;   // y
+      scu[3] = cu;   // A x
+      scu[4] = ct;   // A y
+    }
+    __syncthreads();
+  }
+  // Leave the vectors normalised for the host (all blocks are past the last phase's barrier).
+  {
+    const PersistNorm<R, NC> nx{static_cast<R*>(const_cast<void*>(pa.ps[3].src[0])), vs[0]};
+    const PersistNorm<R, NC> ny{static_cast<R*>(const_cast<void*>(pa.ps[3].src[1])), vs[1]};
+    const PersistNorm<R, NC> nax{static_cast<R*>(const_cast<void*>(pa.ps[3].src[3])), vs[0]};
+    const PersistNorm<R, NC> nay{static_cast<R*>(const_cast<void*>(pa.ps[3].src[4])), vs[1]};
+    const PersistNorm<R, NC> nr{static_cast<R*>(pa.ps[3].out[4]), vs[0]};
+    const int64_t tid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t i = tid; i < pa.n; i += stride) {
+      nx.apply(i);
+      ny.apply(i);
+      nax.apply(i);
+      nay.apply(i);
+      nr.apply(i);
+    }
   }
   if constexpr (CLU) persist_sync<true>(pa, gen);   // no block leaves while others read its smem
   if (blockIdx.x == 0) {
@@ -1682,14 +1766,13 @@ class Locg {
     R *ax = ax_.ptr, *ay = ay_.ptr, *ap = ap_.ptr;
     PersistArgs pa{};
     fill(pa.ps[0], {r, x, y}, {p}, {{100, 100}, {1, 100}, {2, 100}}, P_PROJ_NORM_IPS, G_NONE);
-    fill(pa.ps[1], {p, x, y}, {p}, {}, P_NONE, G_NONE);
     fill(pa.ps[2], {x, y, p, ax, ay, ap}, {},
          {{0, 3}, {1, 4}, {2, 5}, {1, 3}, {2, 3}, {2, 4}, {2, 2}, {1, 2}}, P_GRAM_IMPLICIT,
          G_NONE);
-    fill(pa.ps[3], {x, y, p, ax, ay, ap}, {x, y, ax, ay}, {{100, 100}, {101, 101}},
-         P_UPDATE_NORMS, G_NONE);
-    fill(pa.ps[4], {x, y, ax, ay}, {x, y, ax, ay, r},
-         {{104, 104}, {102, 102}, {100, 104}, {101, 104}}, P_CONV_PROJ, G_NONE);
+    // update pass (PShapeU): unnormalised u, t, A u, A t, r'; the kernel applies the norms
+    fill(pa.ps[3], {x, y, p, ax, ay, ap}, {x, y, ax, ay, r},
+         {{100, 100}, {101, 101}, {104, 104}, {102, 102}, {100, 104}, {101, 104}}, P_NONE,
+         G_NONE);
     pa.row_ptr = op->row_ptr.ptr;
     pa.cols = op->cols.ptr;
     if constexpr (sizeof(R) == 8) pa.vals = op->values.ptr;
