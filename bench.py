@@ -574,10 +574,15 @@ def locg_bytes(n, m, j, p):
     """Algorithmic bytes of one LOCG iteration: matvecs x the matvec formula (W = 1, w_c = 16)
     plus the vector reads and writes of the fused passes, counted from the iteration bodies:
     the FP64 reference iteration (ground_locg.py:324-383) makes 4 complex128 matvecs and 42
-    vector reads/writes; an FP32 sweep of the mixed solver 1 complex64 matvec and 33."""
+    vector reads/writes; an FP32 sweep of the mixed solver 1 complex64 matvec and 33 as a graph
+    of passes, 20 in the persistent launch (operators of at most 4 Mi rows and 64 Mi stored
+    pairs: C1, C5)."""
     def mv(w_v):
         return n * (8 + 2 * w_v) + p * w_v + m * (8 + 16) + j * 8
-    return {'fp64': 4 * mv(16) + 42 * n * 16, 'fp32_sweep': mv(8) + 33 * n * 8,
+    persistent = n <= (4 << 20) and p <= (64 << 20)
+    return {'fp64': 4 * mv(16) + 42 * n * 16,
+            'fp32_sweep': mv(8) + (20 if persistent else 33) * n * 8,
+            'fp32_sweep_form': 'persistent launch' if persistent else 'graph of passes',
             'formula': '#matvecs * (N(8W+2w_v) + P w_v + M(8W+w_c) + 8WJ) + #vector passes * N w_v'}
 
 
@@ -588,10 +593,10 @@ def locg_times(rq, op, wl, dev, use_graph=True):
     # tol=None: the reference default (dtype epsilon in its N-scaled test, ground_locg.py:
     # 224-225, 371-376), i.e. a converged FP64 energy to compare the mixed path against.
     res = {'start_vector': 'complex128 N(0,1)+iN(0,1), normalised', 'tol': None,
-           'timing': 'median of 3 solves per mode after one short warm-up solve',
+           'timing': 'median of 3 solves per mode after one warm-up solve',
            'cuda_graphs': use_graph}
     for mode in ('fp64', 'mixed'):
-        rq.ground_locg(op, x0, maxiter=3, mode=mode, use_graph=use_graph)   # warm-up
+        rq.ground_locg(op, x0, mode=mode, use_graph=use_graph)   # warm-up: a whole solve
         runs = []
         for _ in range(3):
             torch.cuda.synchronize()

@@ -12,6 +12,7 @@
 // CUDA graph with a conditional WHILE node whose condition the convergence step sets.
 //
 // Inner products always accumulate in FP64 (also for FP32 vectors).
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cooperative_groups.h>
@@ -1787,6 +1788,7 @@ class Locg {
     const double avg = n_ > 0 ? static_cast<double>(op->nnz) / static_cast<double>(n_) : 0.0;
     const int lpr = avg >= 96 ? 32 : avg >= 40 ? 16 : avg >= 16 ? 8 : avg >= 6 ? 4
                   : avg >= 2 ? 2 : 1;
+    const auto t_launch = std::chrono::steady_clock::now();
     dispatch_lpr(lpr, [&](auto lpr_t) {
       constexpr int LPR = decltype(lpr_t)::value;
       if constexpr (NC == 2) {
@@ -1801,6 +1803,12 @@ class Locg {
     SQD_CUDA(cudaMemcpyAsync(&fault, bar_.ptr + 2, sizeof(unsigned), cudaMemcpyDeviceToHost,
                              st_));
     SQD_CUDA(cudaStreamSynchronize(st_));
+    if (std::getenv("SQD_LOCG_TRACE"))
+      std::fprintf(stderr, "[sqd_locg persistent] %s, %u blocks (%s), %d iterations, %.3f ms\n",
+                   sizeof(R) == 4 ? "fp32" : "fp64", persist_grid_,
+                   persist_cluster_ ? "cluster" : "cooperative", host_->niter,
+                   std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() -
+                                                             t_launch).count());
     if (fault)
       throw Error(SQD_ERR_DEVICE, "persistent LOCG iteration: a grid barrier timed out");
   }
@@ -2009,8 +2017,14 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, sqd_op_s* cache
   cudaEvent_t ev[5] = {};
   if (trace)
     for (auto& e : ev) SQD_CUDA(cudaEventCreate(&e));
+  // host clock at each mark too: a wait outside this stream's work shows as a gap between the
+  // two clocks
+  std::chrono::steady_clock::time_point th[5];
   auto mark = [&](int k) {
-    if (trace) SQD_CUDA(cudaEventRecord(ev[k], st));
+    if (trace) {
+      SQD_CUDA(cudaEventRecord(ev[k], st));
+      th[k] = std::chrono::steady_clock::now();
+    }
   };
   mark(0);
   constexpr double kInnerRtol = 2e-7;
@@ -2091,10 +2105,15 @@ void run_locg(int64_t n, int dtype, sqd_matvec_fn fn, void* ctx, sqd_op_s* cache
     SQD_CUDA(cudaEventSynchronize(ev[4]));
     float t[4];
     for (int k = 0; k < 4; ++k) SQD_CUDA(cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]));
+    auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+      return std::chrono::duration<double, std::milli>(b - a).count();
+    };
     std::fprintf(stderr,
                  "[sqd_locg mixed] fp32 sweeps %d it %.3f ms | phase switch %.3f ms | "
-                 "fp64 start %.3f ms | fp64 iterations %d it %.3f ms\n",
-                 it32, t[0], t[1], t[2], it64, t[3]);
+                 "fp64 start %.3f ms | fp64 iterations %d it %.3f ms | host %.3f %.3f %.3f "
+                 "%.3f ms\n",
+                 it32, t[0], t[1], t[2], it64, t[3], ms(th[0], th[1]), ms(th[1], th[2]),
+                 ms(th[2], th[3]), ms(th[3], th[4]));
     for (auto& e : ev) cudaEventDestroy(e);
   }
   const LocgDev& h = L.host();
