@@ -604,6 +604,36 @@ struct DotLoop {
   }
 };
 
+// A complex value in a pass's arithmetic type T: float in the FP32 sweeps of the persistent
+// iteration (their outputs are rounded to float, and FP64 arithmetic runs at a fraction of the
+// FP32 rate), double otherwise.  Dots always accumulate in FP64 (a product of two floats is
+// exact in double).
+template <typename T>
+struct C2 {
+  T x, y;
+};
+
+template <int C, typename T>
+__device__ __forceinline__ C2<T> operand_t(const C2<T>* s, const C2<T>* o) {
+  if constexpr (C >= 100) return o[C - 100];
+  else return s[C];
+}
+
+template <typename S, int I, int END>
+struct DotLoopT {
+  template <typename T>
+  __device__ __forceinline__ static void run(double (*acc)[2], const C2<T>* s, const C2<T>* o) {
+    if constexpr (I < END) {
+      const C2<T> xa = operand_t<S::codes[2 * I]>(s, o);
+      const C2<T> ya = operand_t<S::codes[2 * I + 1]>(s, o);
+      const double xr = xa.x, xi = xa.y, yr = ya.x, yi = ya.y;
+      acc[I][0] += xr * yr + xi * yi;   // conj(x) * y
+      acc[I][1] += xr * yi - xi * yr;
+      DotLoopT<S, I + 1, END>::run(acc, s, o);
+    }
+  }
+};
+
 template <typename R, int NC, typename S>
 __global__ void __launch_bounds__(LC_THREADS) k_lcs(LCArgs<6, 10, 5> a) {
   constexpr int NS = S::NS, NO = S::NO, ND = S::ND;
@@ -927,6 +957,18 @@ struct VChunk {
       v[e] = R(t.x);
     }
   }
+  __device__ __forceinline__ C2<R> elem_t(int e, R scale) const {
+    if constexpr (NC == 2) return C2<R>{v[2 * e] * scale, v[2 * e + 1] * scale};
+    else return C2<R>{v[e] * scale, R(0)};
+  }
+  __device__ __forceinline__ void set_t(int e, C2<R> t) {
+    if constexpr (NC == 2) {
+      v[2 * e] = t.x;
+      v[2 * e + 1] = t.y;
+    } else {
+      v[e] = t.x;
+    }
+  }
 };
 static_assert(sizeof(VChunk<float, 2>) == 16 && sizeof(VChunk<float, 1>) == 8 &&
               sizeof(VChunk<double, 1>) == 16 && sizeof(VChunk<double, 2>) == 16, "chunks");
@@ -949,8 +991,8 @@ __device__ __forceinline__ void st_chunk(R* p, int64_t j, const VChunk<R, NC>& c
 }
 
 // One elementwise pass: every element's NO outputs as combinations of its NS sources (each
-// times its scale sc[k], see k_locg_persist) with the coefficients in sd.coef, the ND dots,
-// then the phase end and the post step.  Each thread step moves two elements of every vector
+// times its scale sc[k], see k_locg_persist) with the coefficients in sd.coef, in the vectors'
+// precision, the ND dots in FP64, then the phase end and the post step.  Each thread step moves two elements of every vector
 // (one complex128; 16 bytes for complex64), which puts twice the bytes in flight per load as
 // one element at a time; the vectors are 16-byte aligned (the host checks), an odd last
 // element is done on its own.
@@ -961,20 +1003,31 @@ __device__ __forceinline__ bool persist_pass(const LCArgs<6, 10, 5>& a, LocgDev&
   constexpr int NS = S::NS, NO = S::NO, ND = S::ND;
   constexpr int NOA = NO > 0 ? NO : 1, NDA = ND > 0 ? ND : 1;
   constexpr int VW = VChunk<R, NC>::VW;
+  using T = R;   // the combinations' arithmetic type (C2 above)
+  __shared__ C2<T> co[NOA][NS];
+  for (int t = threadIdx.x; t < NO * NS; t += blockDim.x)
+    co[t / NS][t % NS] = C2<T>{T(sd.coef[t / NS][t % NS][0]), T(sd.coef[t / NS][t % NS][1])};
+  T scl[NS];
+#pragma unroll
+  for (int k = 0; k < NS; ++k) scl[k] = T(sc[k]);
+  __syncthreads();
   double acc[NDA][2];
 #pragma unroll
   for (int d = 0; d < NDA; ++d) acc[d][0] = acc[d][1] = 0.0;
-  auto combine = [&](const double2* sv, double2* ov) {
+  auto combine = [&](const C2<T>* sv, C2<T>* ov) {
 #pragma unroll
     for (int q = 0; q < NO; ++q) {
-      double2 t = make_double2(0.0, 0.0);
+      C2<T> t{T(0), T(0)};
 #pragma unroll
-      for (int k = 0; k < NS; ++k)
-        t = cadd(t, cmul(make_double2(sd.coef[q][k][0], sd.coef[q][k][1]), sv[k]));
-      if constexpr (NC == 1) t.y = 0.0;
+      for (int k = 0; k < NS; ++k) {
+        const C2<T> c = co[q][k];
+        t.x += c.x * sv[k].x - c.y * sv[k].y;
+        t.y += c.x * sv[k].y + c.y * sv[k].x;
+      }
+      if constexpr (NC == 1) t.y = T(0);
       ov[q] = t;
     }
-    DotLoop<S, 0, ND>::run(acc, sv, ov);
+    DotLoopT<S, 0, ND>::run(acc, sv, ov);
   };
   const int64_t tid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
@@ -992,12 +1045,12 @@ __device__ __forceinline__ bool persist_pass(const LCArgs<6, 10, 5>& a, LocgDev&
     VChunk<R, NC> res[NOA];
 #pragma unroll
     for (int e = 0; e < VW; ++e) {
-      double2 sv[NS], ov[NOA];
+      C2<T> sv[NS], ov[NOA];
 #pragma unroll
-      for (int k = 0; k < NS; ++k) sv[k] = cscale(raw[k].elem(e), sc[k]);
+      for (int k = 0; k < NS; ++k) sv[k] = raw[k].elem_t(e, scl[k]);
       combine(sv, ov);
 #pragma unroll
-      for (int q = 0; q < NO; ++q) res[q].set(e, ov[q]);
+      for (int q = 0; q < NO; ++q) res[q].set_t(e, ov[q]);
     }
 #pragma unroll
     for (int q = 0; q < NO; ++q)
@@ -1005,17 +1058,17 @@ __device__ __forceinline__ bool persist_pass(const LCArgs<6, 10, 5>& a, LocgDev&
   }
   if constexpr (VW > 1) {
     for (int64_t i = nvec * VW + tid; i < a.n; i += stride) {
-      double2 sv[NS], ov[NOA];
+      C2<T> sv[NS], ov[NOA];
 #pragma unroll
       for (int k = 0; k < NS; ++k) {
         const Cx<R> v = ld_elem_cg<R, NC>(static_cast<const R*>(a.src[k]), i);
-        sv[k] = cscale(make_double2(double(v.re), double(v.im)), sc[k]);
+        sv[k] = C2<T>{v.re * scl[k], v.im * scl[k]};
       }
       combine(sv, ov);
 #pragma unroll
       for (int q = 0; q < NO; ++q)
         if (a.out[q] != nullptr)
-          st_elem<R, NC>(static_cast<R*>(a.out[q]), i, cx_make<R>(R(ov[q].x), R(ov[q].y)));
+          st_elem<R, NC>(static_cast<R*>(a.out[q]), i, cx_make<R>(ov[q].x, ov[q].y));
     }
   }
   if (!persist_finish<ND, CLU>(acc, sd, pa, gen, cpart, buf)) return false;
