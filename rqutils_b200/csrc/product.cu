@@ -351,9 +351,11 @@ k_slab2(int64_t A, int64_t B, int64_t total_k, int64_t a_tiles, const int64_t* _
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t panels = (B + 63) >> 6;
   // element chunk of a step (4 x 64 entries, 1 or 2 KB) prefetched into L2 about 2 KB ahead,
-  // as in k_slab (C3 FP32 matvec 3.32 -> 2.78 ms, C2 0.234 -> 0.210 ms; 1 KB ahead: 2.95 ms)
-  constexpr int kChunkLines = 4 * 64 * NCA * static_cast<int>(sizeof(R)) / 128;
-  constexpr int pv = kChunkLines >= 16 ? 1 : 16 / kChunkLines;
+  // as in k_slab (C3 FP32 matvec 3.32 -> 2.78 ms, C2 0.234 -> 0.210 ms; 1 KB ahead: 2.95 ms);
+  // in the first pass only: the final pass, which also reads both FP64 partials, measured
+  // slower with it (c3_small 90.5 -> 104.9 us, C3 1171 -> 1295 us)
+  constexpr int kChunkLines = FINAL ? 0 : 4 * 64 * NCA * static_cast<int>(sizeof(R)) / 128;
+  constexpr int pv = kChunkLines >= 16 ? 1 : kChunkLines > 0 ? 16 / kChunkLines : 1;
   for (int64_t blk = blockIdx.x; blk < panels * a_tiles; blk += gridDim.x) {
     const int64_t p = blk / a_tiles;
     const int64_t a = (blk - p * a_tiles) * 8 + warp;
